@@ -1,0 +1,153 @@
+/*
+ * gt.h -- C ABI of libgt, the B200 (sm_100a) locate-and-link library.
+ *
+ * Drop-in boundary for gpu_tracking's hot path.  Each entry point names the
+ * reference interface it replaces (paths relative to the reference repo
+ * amfaber/tracking_optimizations):
+ *
+ *   gt_batch           gpu-tracking/src/lib.rs:46-121 `batch_rust`
+ *                      -> execute_gpu.rs:496-508 `execute_ndarray`
+ *                      -> execute_gpu.rs:372-494 `execute_gpu`
+ *   gt_batch_device    same computation on device-resident frames; the
+ *                      result table stays on the device
+ *   gt_link            gpu-tracking/src/lib.rs:202-212 `link_rust`
+ *                      -> linking.rs:570-580 `linker_all` over
+ *                      linking.rs:12-61 `FrameSubsetter`
+ *   gt_column_names    execute_gpu.rs:197-226 `column_names`
+ *
+ * Conventions: plain pointers and sizes, no C++ or torch types.  Every call
+ * returns a gt_status; on failure gt_last_error() describes it.  A context
+ * is bound to one device, owns one CUDA stream and is not thread-safe.
+ * Input pointers are borrowed for the duration of the call.
+ */
+#ifndef GT_H
+#define GT_H
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GT_API __attribute__((visibility("default")))
+#else
+#define GT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gt_status {
+    GT_OK = 0,
+    GT_ERR_ARG = 1,             /* invalid argument (shape, dtype, range) */
+    GT_ERR_CUDA = 2,            /* CUDA runtime error */
+    GT_ERR_OOM = 3,             /* device allocation failed */
+    GT_ERR_SUBNET_BUDGET = 4,   /* a linking subnetwork exceeded the search budget */
+    GT_ERR_DEVICE_TIMEOUT = 5,  /* a bounded device wait expired */
+    GT_ERR_UNSUPPORTED = 6,     /* parameter the reference rejects (lib.rs:73-74) */
+    GT_ERR_CAPACITY = 7         /* a per-frame capacity was exceeded after retries */
+} gt_status;
+
+typedef enum gt_dtype { GT_U16 = 0, GT_F32 = 1 } gt_dtype;
+
+/* The 21 keyword arguments of gpu_tracking.batch (gpu_tracking/lib.py:6-28),
+ * each Option<> carried as a has_* flag (0 = None).  Defaults are applied as
+ * lib.rs:77-91 does. */
+typedef struct gt_params {
+    uint32_t diameter;
+    int32_t has_minmass;        float minmass;
+    int32_t has_maxsize;        float maxsize;
+    int32_t has_separation;     uint32_t separation;
+    int32_t has_noise_size;     float noise_size;
+    int32_t has_smoothing_size; uint32_t smoothing_size;
+    int32_t has_threshold;      float threshold;
+    int32_t has_invert;         int32_t invert;
+    int32_t has_percentile;     float percentile;
+    int32_t has_topn;           uint32_t topn;
+    int32_t has_preprocess;     int32_t preprocess;
+    int32_t has_max_iterations; uint32_t max_iterations;
+    int32_t has_characterize;   int32_t characterize;
+    int32_t has_filter_close;   int32_t filter_close;
+    int32_t has_search_range;   float search_range;
+    int32_t has_memory;         uint32_t memory;
+    int32_t has_cpu_processed;  int32_t cpu_processed;
+    int32_t has_sig_radius;     float sig_radius;
+    int32_t has_bg_radius;      float bg_radius;
+    int32_t has_gap_radius;     float gap_radius;
+} gt_params;
+
+#define GT_MAX_COLS 16
+
+/* Result of gt_batch: nrows x ncols row-major f32 (the reference returns the
+ * same matrix plus its column list, lib.rs:119-120).  `data` is owned by the
+ * library; release it with gt_table_free. */
+typedef struct gt_table {
+    float* data;
+    int64_t nrows;
+    int32_t ncols;
+    char names[GT_MAX_COLS][24];
+    char types[GT_MAX_COLS][8];
+} gt_table;
+
+typedef struct gt_ctx gt_ctx;
+
+/* Library version string. */
+GT_API const char* gt_version(void);
+
+/* Create a context on CUDA device `device`. */
+GT_API int gt_ctx_create(int device, gt_ctx** out);
+
+/* Destroy a context and free its device memory. */
+GT_API void gt_ctx_destroy(gt_ctx* ctx);
+
+/* Description of the last failure on this context ("" if none); with a NULL
+ * context, the last failure of a context-free call on this thread. */
+GT_API const char* gt_last_error(const gt_ctx* ctx);
+
+/* Column names/types for a parameter set: "frame:int,mass:float,...".
+ * Returns the number of columns, or a negative gt_status. */
+GT_API int gt_column_names(const gt_params* params, char* buf, size_t buflen);
+
+/* Locate (and link when has_search_range) T frames of H x W pixels held in
+ * HOST memory (u16 or f32, C-contiguous).  Host->device and device->host
+ * copies happen inside the call.  Replaces batch_rust / execute_ndarray. */
+GT_API int gt_batch(gt_ctx* ctx, const void* frames, int dtype, int T, int H, int W,
+             const gt_params* params, gt_table* out);
+
+/* Same on DEVICE-resident frames.  The table is written to the device
+ * buffer `d_out` (capacity out_rows x ncols floats); *nrows receives the row
+ * count (rows beyond out_rows are not written, *nrows still reports them).
+ * `stream` is a cudaStream_t (NULL = the context's stream); the call
+ * returns after the work on it has finished. */
+GT_API int gt_batch_device(gt_ctx* ctx, const void* d_frames, int dtype, int T, int H, int W,
+                    const gt_params* params, float* d_out, int64_t out_rows,
+                    int64_t* nrows, void* stream);
+
+/* Link an (n x ncols) host f32 table whose columns 0, 2, 3 are frame, y, x
+ * (link_rust's FrameSubsetter layout).  Writes n trajectory IDs. */
+GT_API int gt_link(gt_ctx* ctx, const float* rows, int64_t n, int ncols, float search_range,
+            int has_memory, uint32_t memory, uint64_t* ids);
+
+/* Free a table returned by gt_batch. */
+GT_API void gt_table_free(gt_table* table);
+
+/* Statistics of the last call on this context: fixed-point iterations of the
+ * memory linker, fallback walks, candidates and particles. */
+typedef struct gt_stats {
+    int32_t link_iterations;   /* fixed-point passes of the memory linker */
+    int32_t fallback_walks;    /* walks that left a tile's halo */
+    int64_t candidates;        /* located features before the separation filter */
+    int64_t particles;         /* rows of the output table */
+    int32_t retries;           /* capacity retries */
+    int32_t launches;          /* kernels launched by the call */
+    float ms_locate;           /* device time of the locate kernel(s) */
+    float ms_finalize;         /* fallback walks + ordering + separation filter */
+    float ms_link;             /* linking incl. fixed-point passes and ids */
+    float ms_assemble;         /* output table */
+    float ms_total;            /* first to last kernel of the call */
+} gt_stats;
+
+GT_API int gt_last_stats(const gt_ctx* ctx, gt_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GT_H */

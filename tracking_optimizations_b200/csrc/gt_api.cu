@@ -1,0 +1,853 @@
+// gt_api.cu -- host side of libgt: parameter derivation, workspace, launch
+// sequence and the extern "C" entry points declared in include/gt.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gt.h"
+#include "gt_internal.cuh"
+
+namespace gt {
+__global__ void locate_tiles_kernel(const LocParams p, const MovieBufs b, int frame0);
+__global__ void fallback_walk_kernel(const LocParams p, const MovieBufs b, int win);
+__global__ void finalize_kernel(const LocParams p, MovieBufs b, float sep, int link_grid);
+__global__ void link_frames_kernel(LinkBufs L, int only_dirty);
+__global__ void memory_kernel(LinkBufs L, int memory);
+__global__ void root_init_kernel(LinkBufs L, const int* total);
+__global__ void root_jump_kernel(LinkBufs L, const int* total);
+__global__ void scan_frames_kernel(const int* in, int* out, int n);
+__global__ void newid_kernel(const int* newrank, const int* newbase, const int* off, const int* npart,
+                             int* newid, int T);
+__global__ void assemble_kernel(AsmArgs a);
+__global__ void grid_kernel(const float* py, const float* px, const int* npart, int cap_p, int G,
+                            int ncy, int ncx, int* gstart, int* gidx);
+}  // namespace gt
+
+using namespace gt;
+
+struct gt_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    char* arena = nullptr;
+    size_t arena_size = 0;
+    gt_stats stats{};
+    int num_sms = 148;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+constexpr int LOC_TH = 32;
+constexpr int LOC_TW = 64;
+constexpr int LOC_CMAX = 512;
+constexpr int FB_WIN_MAX = 100;
+constexpr long long SUBNET_BUDGET = 1LL << 26;  // option trials per subnet
+
+struct Resolved {
+    // lib.rs:77-91 defaults
+    uint32_t diameter;
+    float minmass;
+    uint32_t separation;
+    float noise_size;
+    uint32_t smoothing_size;
+    uint32_t max_iterations;
+    int characterize;
+    int cpu_processed;
+    int has_search_range;
+    float search_range;
+    uint32_t memory;
+    int has_sig, has_bg;
+    float sig_radius, bg_radius, gap_radius;
+};
+
+int resolve(const gt_params* p, Resolved* r, std::string* msg) {
+    // lib.rs:73-74 not_implemented!(maxsize, threshold, invert, percentile, topn, preprocess)
+    const char* ni = nullptr;
+    if (p->has_maxsize) ni = "maxsize";
+    else if (p->has_threshold) ni = "threshold";
+    else if (p->has_invert) ni = "invert";
+    else if (p->has_percentile) ni = "percentile";
+    else if (p->has_topn) ni = "topn";
+    else if (p->has_preprocess) ni = "preprocess";
+    if (ni) { *msg = std::string(ni) + " is not implemented"; return GT_ERR_UNSUPPORTED; }
+    r->diameter = p->diameter;
+    r->minmass = p->has_minmass ? p->minmass : 0.0f;
+    r->separation = p->has_separation ? p->separation : p->diameter + 1;
+    r->noise_size = p->has_noise_size ? p->noise_size : 1.0f;
+    r->smoothing_size = p->has_smoothing_size ? p->smoothing_size : p->diameter;
+    r->max_iterations = p->has_max_iterations ? p->max_iterations : 10;
+    r->characterize = p->has_characterize ? (p->characterize != 0) : 0;
+    r->cpu_processed = p->has_cpu_processed ? (p->cpu_processed != 0) : 0;
+    r->has_search_range = p->has_search_range;
+    r->search_range = p->search_range;
+    r->memory = p->has_memory ? p->memory : 0;  // Linker::new(range, memory.unwrap_or(0))
+    r->has_sig = p->has_sig_radius;
+    r->sig_radius = p->sig_radius;
+    r->has_bg = p->has_bg_radius;
+    r->bg_radius = p->bg_radius;
+    r->gap_radius = p->has_gap_radius ? p->gap_radius : 0.0f;  // lib.rs:91
+    if (r->has_bg && !r->has_sig) {
+        // execute_gpu.rs:301-333 only gathers raw pixels when sig_radius is
+        // set; the reference then fails reshaping its output.
+        *msg = "bg_radius requires sig_radius";
+        return GT_ERR_ARG;
+    }
+    if (r->smoothing_size < 1 || r->smoothing_size / 2 * 2 + 1 > GT_MAX_TAPS) {
+        *msg = "smoothing_size must be in [1, 63]";
+        return GT_ERR_ARG;
+    }
+    if (r->diameter > 63) { *msg = "diameter must be <= 63"; return GT_ERR_ARG; }
+    if (r->separation > 4096) { *msg = "separation must be <= 4096"; return GT_ERR_ARG; }
+    if (r->has_search_range && !(r->search_range > 0.0f && r->search_range < 4096.0f)) {
+        *msg = "search_range must be in (0, 4096)";
+        return GT_ERR_ARG;
+    }
+    if (r->memory > 1000) { *msg = "memory must be <= 1000"; return GT_ERR_ARG; }
+    return GT_OK;
+}
+
+void column_list(const Resolved& r, std::vector<std::string>& names, std::vector<std::string>& types) {
+    // execute_gpu.rs:197-226
+    names = {"frame", "mass", "y", "x"};
+    types = {"int", "float", "float", "float"};
+    if (r.has_search_range) { names.push_back("particle"); types.push_back("int"); }
+    if (r.cpu_processed) for (auto n : {"Rg", "ecc", "signal"}) { names.push_back(n); types.push_back("float"); }
+    if (r.has_sig) { names.push_back("raw_mass"); types.push_back("float"); }
+    if (r.has_bg) for (auto n : {"raw_bg_median", "raw_mass_corrected"}) { names.push_back(n); types.push_back("float"); }
+    if (r.characterize)
+        for (auto n : {"Rg_gpu", "raw_mass_gpu", "signal_gpu", "ecc_gpu"}) { names.push_back(n); types.push_back("float"); }
+}
+
+// gpu_setup.rs:48 dilation and max_rows.wgsl:17 offset
+void dilation(uint32_t sep, int* D, int* o) {
+    float v = (2.0f * (float)sep) / std::sqrt(2.0f);
+    unsigned d = v <= 0.0f ? 0u : (unsigned)v;
+    float half = (float)(int)d / 2.0f - 0.5f;
+    *D = (int)d;
+    *o = (int)half;
+}
+
+int next_pow2(long long x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+struct Plan {
+    int T = 0, H = 0, W = 0, dtype = 0;
+    Resolved r{};
+    LocParams lp{};
+    float sep = 0.f;
+    int link = 0;
+    int cap_c = 0, cap_p = 0, cap_m = 0, cap_s = 0, cap_e = 0;
+    int G = 8, ncx = 1, ncy = 1;
+    int nslot = 1, hsize = 64;
+    size_t smem_loc = 0, smem_fb = 0, smem_fin = 0;
+    int fb_win = 0;
+    std::vector<float> char_tab, gchar_tab;
+    std::vector<int> char_off, sig_off, bg_off;
+    std::vector<std::string> names, types;
+};
+
+void circle_tables(int R, std::vector<float>& tab, std::vector<int>* off, int stride3) {
+    // kernels.rs:134-150, 169-206: i outer (row), j inner (column)
+    for (int i = -R; i <= R; ++i)
+        for (int j = -R; j <= R; ++j)
+            if (i * i + j * j <= R * R) {
+                float th = std::atan2((float)j, (float)i);
+                if (stride3) tab.push_back((float)(i * i + j * j));
+                tab.push_back(std::sin(2.0f * th));
+                tab.push_back(std::cos(2.0f * th));
+                if (off) { off->push_back(i); off->push_back(j); }
+            }
+}
+
+void circle_inds_f(float radius, std::vector<int>& off) {
+    // kernels.rs:134-150 with a float radius
+    int rb = (int)std::ceil(radius);
+    float r2 = radius * radius;
+    for (int i = -rb; i <= rb; ++i)
+        for (int j = -rb; j <= rb; ++j)
+            if ((float)(i * i + j * j) <= r2) { off.push_back(i); off.push_back(j); }
+}
+
+void annulus_inds_f(float outer, float inner, std::vector<int>& off) {
+    // kernels.rs:152-167
+    int b = (int)std::ceil(outer);
+    float or2 = outer * outer, ir2 = inner * inner;
+    for (int i = -b; i <= b; ++i)
+        for (int j = -b; j <= b; ++j) {
+            float r2 = (float)(i * i + j * j);
+            if (r2 <= or2 && r2 >= ir2) { off.push_back(i); off.push_back(j); }
+        }
+}
+
+int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int num_sms, Plan* pl,
+              std::string* msg) {
+    Plan& P = *pl;
+    P.T = T; P.H = H; P.W = W; P.dtype = dtype; P.r = r;
+    LocParams& lp = P.lp;
+    std::memset(&lp, 0, sizeof(lp));
+    lp.H = H; lp.W = W;
+    const int k = (int)r.smoothing_size;
+    lp.krad = k / 2;
+    lp.taps = 2 * lp.krad + 1;
+    if (H <= lp.krad || W <= lp.krad) { *msg = "frame smaller than the smoothing window"; return GT_ERR_ARG; }
+    // preprocess_rows.wgsl:44-45 weights and their running sum
+    const float sigma2 = r.noise_size;
+    float norm = 0.0f;
+    for (int i = -lp.krad; i <= lp.krad; ++i) {
+        const float x = (float)i;
+        const float g = std::exp(-x * x / (2.0f * sigma2));
+        lp.w[i + lp.krad] = g;
+        norm = norm + g;
+    }
+    lp.norm = norm;
+    lp.kk = (float)(k * k);
+    dilation(r.separation, &lp.D, &lp.o);
+    lp.d = (int)r.diameter;
+    lp.rint_c = ((int)r.diameter - 1) / 2;
+    lp.border = (int)r.diameter / 2;
+    lp.char_r = (int)r.diameter / 2;
+    lp.max_iter = (int)r.max_iterations;
+    lp.thr = 0.6f;  // gpu_setup.rs:57
+    lp.minmass = r.minmass;
+    lp.hp = std::max({lp.o, lp.D - 1 - lp.o, lp.char_r, lp.rint_c + 2, 1});
+    lp.TH = LOC_TH; lp.TW = LOC_TW;
+    lp.ntx = (W + lp.TW - 1) / lp.TW;
+    lp.nty = (H + lp.TH - 1) / lp.TH;
+    lp.dtype = dtype;
+    lp.cpu_processed = r.cpu_processed;
+    lp.characterize = r.characterize;
+    lp.zero_skip = lp.max_iter >= 1 && lp.rint_c <= lp.o && lp.rint_c <= lp.D - 1 - lp.o;
+    P.char_tab.clear(); P.char_off.clear(); P.gchar_tab.clear();
+    circle_tables(lp.char_r, P.char_tab, &P.char_off, 1);
+    circle_tables(lp.rint_c, P.gchar_tab, nullptr, 0);
+    lp.n_char = (int)P.char_off.size() / 2;
+    lp.n_gchar = (int)P.gchar_tab.size() / 2;
+    P.sig_off.clear(); P.bg_off.clear();
+    if (r.has_sig) circle_inds_f(r.sig_radius, P.sig_off);
+    if (r.has_bg) annulus_inds_f(r.bg_radius, r.sig_radius + r.gap_radius, P.bg_off);
+    P.sep = (float)r.separation;
+    P.link = r.has_search_range;
+
+    const int PH = lp.TH + 2 * lp.hp, PW = lp.TW + 2 * lp.hp;
+    const int RH = PH + 2 * lp.krad, RW = PW + 2 * lp.krad;
+    P.smem_loc = sizeof(float) * ((size_t)RH * RW + 2 * (size_t)RH * PW + (size_t)PH * PW) +
+                 sizeof(int) * (size_t)lp.TH * lp.TW + 4 * sizeof(float) * LOC_CMAX + (size_t)lp.TH * lp.TW;
+    P.smem_loc = (P.smem_loc + 15) / 16 * 16;
+    if (P.smem_loc > 227 * 1024) { *msg = "diameter/separation too large for the tile plan"; return GT_ERR_ARG; }
+    P.fb_win = std::min(FB_WIN_MAX, std::max(lp.rint_c + 1, lp.max_iter - 1 + lp.rint_c + 1));
+    P.smem_fb = sizeof(float) * (size_t)(2 * P.fb_win + 1) * (2 * P.fb_win + 1);
+
+    // capacities (bounds; overflow is detected on the device and retried)
+    const long long HW = (long long)H * W;
+    long long cc = std::max<long long>(4096, HW / 64) * scale;
+    P.cap_c = (int)std::min<long long>(cc, std::max<long long>(HW, 1));
+    const double s = std::max(1.0f, P.sep);
+    const double ext_h = H + 2.0 * lp.rint_c + s, ext_w = W + 2.0 * lp.rint_c + s;
+    long long pack = (long long)(ext_h * ext_w / (0.785 * s * s)) + 16;
+    P.cap_p = (int)std::min<long long>(P.cap_c, pack * scale);
+    P.cap_m = (int)std::max<long long>(1, (long long)r.memory * P.cap_p);
+    P.cap_s = P.cap_p + P.cap_m;
+    const double sr = P.link ? r.search_range : 1.0;
+    long long deg = (long long)((2 * sr + s) * (2 * sr + s) / (0.785 * s * s)) + 2;
+    P.cap_e = (int)std::min<long long>((long long)P.cap_s * std::min<long long>(deg * scale, P.cap_p),
+                                       (long long)1 << 30);
+    P.G = std::max({(int)std::ceil(P.sep) + 1, P.link ? (int)std::ceil(r.search_range) + 1 : 0, 8,
+                    (int)std::ceil(std::sqrt((double)HW / 16384.0))});
+    P.ncy = (H + P.G - 1) / P.G;
+    P.ncx = (W + P.G - 1) / P.G;
+    P.smem_fin = sizeof(int) * (size_t)P.ncx * P.ncy;
+    if (P.smem_fin > 200 * 1024) { *msg = "grid too fine"; return GT_ERR_ARG; }
+    P.hsize = 2 * next_pow2(2LL * std::max({P.cap_p, P.cap_m, 32}));
+    // link slots: bounded scratch
+    const size_t nn = (size_t)P.cap_s + P.cap_p;
+    const size_t per_slot = 4 * (3 * (size_t)P.cap_s + 1) + 8 * (size_t)P.cap_e * 2 + 4 * ((size_t)P.cap_p + 1) +
+                            4 * 4 * nn + nn + 16 * nn + 4 + 8 * (size_t)P.hsize;
+    const size_t budget = (size_t)6 << 30;
+    P.nslot = (int)std::max<size_t>(1, std::min<size_t>({(size_t)T, (size_t)num_sms * 4, budget / per_slot}));
+    column_list(r, P.names, P.types);
+    return GT_OK;
+}
+
+// Device workspace carved from one arena.
+struct Work {
+    void* frames;
+    Cand* cand;
+    int *fcount, *rowcnt, *pend, *npend;
+    float *py, *px, *pm;
+    int *prec, *npart, *gstart, *gidx;
+    int *cperm, *crec, *ccell, *cstart, *cidx;
+    float *cy, *cx, *cm;
+    float *char_tab, *gchar_tab;
+    int *char_off, *sig_off, *bg_off;
+    int* err;
+    int *off, *pred, *mlist, *mcount, *dirty, *ndirty, *newrank, *newcount, *newbase, *root, *newid;
+    unsigned char* lnext;
+    float *s_y, *s_x, *e_w, *d_w;
+    int *s_h, *s_deg, *e_dst, *d_cnt, *d_src, *uf, *c_nd, *c_ns, *c_min, *work, *bump, *hkey, *hval;
+    unsigned char* vis;
+    float* out;
+};
+
+struct Carver {
+    char* base;
+    size_t off = 0;
+    template <class X>
+    X* take(size_t n) {
+        off = (off + 255) / 256 * 256;
+        X* p = (X*)(base ? base + off : nullptr);
+        off += sizeof(X) * std::max<size_t>(n, 1);
+        return p;
+    }
+};
+
+size_t carve(const Plan& P, char* base, Work* w, size_t frame_bytes, bool need_locate) {
+    Carver c{base};
+    const size_t T = P.T;
+    const size_t ncell = (size_t)P.ncx * P.ncy;
+    w->frames = c.take<char>(frame_bytes);
+    const size_t cc = need_locate ? T * P.cap_c : 1;
+    w->cand = c.take<Cand>(cc);
+    w->fcount = c.take<int>(T);
+    w->rowcnt = c.take<int>(need_locate ? T * P.H * P.lp.ntx : 1);
+    w->pend = c.take<int>(cc);
+    w->npend = c.take<int>(1);
+    w->py = c.take<float>(T * P.cap_p);
+    w->px = c.take<float>(T * P.cap_p);
+    w->pm = c.take<float>(T * P.cap_p);
+    w->prec = c.take<int>(T * P.cap_p);
+    w->npart = c.take<int>(T);
+    w->gstart = c.take<int>(T * (ncell + 1));
+    w->gidx = c.take<int>(T * P.cap_p);
+    w->cperm = c.take<int>(cc);
+    w->crec = c.take<int>(cc);
+    w->ccell = c.take<int>(cc);
+    w->cstart = c.take<int>(need_locate ? T * (ncell + 1) : 1);
+    w->cidx = c.take<int>(cc);
+    w->cy = c.take<float>(cc);
+    w->cx = c.take<float>(cc);
+    w->cm = c.take<float>(cc);
+    w->char_tab = c.take<float>(P.char_tab.size());
+    w->gchar_tab = c.take<float>(P.gchar_tab.size());
+    w->char_off = c.take<int>(P.char_off.size());
+    w->sig_off = c.take<int>(P.sig_off.size());
+    w->bg_off = c.take<int>(P.bg_off.size());
+    w->err = c.take<int>(4);
+    w->off = c.take<int>(T + 1);
+    const size_t np = P.link ? T * P.cap_p : 1;
+    w->pred = c.take<int>(np);
+    w->lnext = c.take<unsigned char>(np);
+    w->mlist = c.take<int>(P.link ? T * P.cap_m : 1);
+    w->mcount = c.take<int>(T);
+    w->dirty = c.take<int>(T);
+    w->ndirty = c.take<int>(1);
+    w->newrank = c.take<int>(np);
+    w->newcount = c.take<int>(T);
+    w->newbase = c.take<int>(T + 1);
+    w->root = c.take<int>(np);
+    w->newid = c.take<int>(np);
+    const size_t S = P.link ? P.nslot : 0;
+    const size_t nn = (size_t)P.cap_s + P.cap_p;
+    w->s_y = c.take<float>(S * P.cap_s);
+    w->s_x = c.take<float>(S * P.cap_s);
+    w->s_h = c.take<int>(S * P.cap_s);
+    w->s_deg = c.take<int>(S * (P.cap_s + 1));
+    w->e_dst = c.take<int>(S * P.cap_e);
+    w->e_w = c.take<float>(S * P.cap_e);
+    w->d_cnt = c.take<int>(S * (P.cap_p + 1));
+    w->d_src = c.take<int>(S * P.cap_e);
+    w->d_w = c.take<float>(S * P.cap_e);
+    w->uf = c.take<int>(S * nn);
+    w->c_nd = c.take<int>(S * nn);
+    w->c_ns = c.take<int>(S * nn);
+    w->c_min = c.take<int>(S * nn);
+    w->vis = c.take<unsigned char>(S * nn);
+    w->work = c.take<int>(S * 4 * nn);
+    w->bump = c.take<int>(S);
+    w->hkey = c.take<int>(S * P.hsize);
+    w->hval = c.take<int>(S * P.hsize);
+    w->out = c.take<float>(need_locate ? T * P.cap_p * P.names.size() : 1);
+    return c.off + 256;
+}
+
+#define CK(x)                                                                              \
+    do {                                                                                   \
+        cudaError_t e_ = (x);                                                              \
+        if (e_ != cudaSuccess) {                                                           \
+            ctx->err = std::string(#x) + ": " + cudaGetErrorString(e_);                    \
+            return e_ == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA;             \
+        }                                                                                  \
+    } while (0)
+
+int ensure_arena(gt_ctx* ctx, size_t bytes) {
+    if (ctx->arena_size >= bytes) return GT_OK;
+    if (ctx->arena) { cudaFree(ctx->arena); ctx->arena = nullptr; ctx->arena_size = 0; }
+    size_t want = bytes + bytes / 8;
+    CK(cudaMalloc((void**)&ctx->arena, want));
+    ctx->arena_size = want;
+    return GT_OK;
+}
+
+LinkBufs link_bufs(const Plan& P, const Work& w) {
+    LinkBufs L{};
+    L.T = P.T; L.cap_p = P.cap_p; L.cap_m = P.cap_m; L.cap_e = P.cap_e; L.cap_s = P.cap_s;
+    L.r = P.r.search_range;
+    L.G = P.G; L.ncx = P.ncx; L.ncy = P.ncy;
+    L.py = w.py; L.px = w.px; L.npart = w.npart; L.off = w.off; L.gstart = w.gstart; L.gidx = w.gidx;
+    L.pred = w.pred; L.lnext = w.lnext; L.mlist = w.mlist; L.mcount = w.mcount; L.dirty = w.dirty;
+    L.ndirty = w.ndirty; L.newrank = w.newrank; L.newcount = w.newcount; L.root = w.root; L.err = w.err;
+    L.budget = SUBNET_BUDGET;
+    L.nslot = P.nslot;
+    L.s_y = w.s_y; L.s_x = w.s_x; L.s_h = w.s_h; L.s_deg = w.s_deg; L.e_dst = w.e_dst; L.e_w = w.e_w;
+    L.d_cnt = w.d_cnt; L.d_src = w.d_src; L.d_w = w.d_w; L.uf = w.uf; L.c_nd = w.c_nd; L.c_ns = w.c_ns;
+    L.c_min = w.c_min; L.vis = w.vis; L.work = w.work; L.bump = w.bump; L.hkey = w.hkey; L.hval = w.hval;
+    L.hsize = P.hsize;
+    return L;
+}
+
+// Linking over the particle tables already in the workspace (npart, py, px,
+// gstart/gidx, off).  Leaves trajectory ids in newid[root[g]].
+int run_link(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
+    LinkBufs L = link_bufs(P, w);
+    const int T = P.T;
+    CK(cudaMemsetAsync(w.mcount, 0, sizeof(int) * T, st));
+    CK(cudaMemsetAsync(w.dirty, 0, sizeof(int) * T, st));
+    link_frames_kernel<<<P.nslot, 256, 0, st>>>(L, 0);
+    CK(cudaGetLastError());
+    ctx->stats.launches += 1;
+    int rounds = 1;
+    while ((1 << rounds) < T + 1) ++rounds;
+    rounds += 1;
+    const int rblocks = ctx->num_sms * 8;
+    auto roots = [&]() -> int {
+        root_init_kernel<<<rblocks, 256, 0, st>>>(L, w.off + T);
+        for (int i = 0; i < rounds; ++i) root_jump_kernel<<<rblocks, 256, 0, st>>>(L, w.off + T);
+        CK(cudaGetLastError());
+        ctx->stats.launches += 1 + rounds;
+        return GT_OK;
+    };
+    int iters = 0;
+    if (P.r.memory > 0 && T > 2) {
+        for (iters = 1; iters <= T + 1; ++iters) {
+            int rc = roots();
+            if (rc) return rc;
+            CK(cudaMemsetAsync(w.ndirty, 0, sizeof(int), st));
+            memory_kernel<<<P.nslot, 256, 0, st>>>(L, (int)P.r.memory);
+            CK(cudaGetLastError());
+            ctx->stats.launches += 1;
+            int nd = 0;
+            CK(cudaMemcpyAsync(&nd, w.ndirty, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (nd == 0) break;
+            link_frames_kernel<<<P.nslot, 256, 0, st>>>(L, 1);
+            CK(cudaGetLastError());
+            ctx->stats.launches += 1;
+        }
+    }
+    ctx->stats.link_iterations = iters;
+    int rc = roots();
+    if (rc) return rc;
+    scan_frames_kernel<<<1, 1024, 0, st>>>(w.newcount, w.newbase, T);
+    newid_kernel<<<T, 256, 0, st>>>(w.newrank, w.newbase, w.off, w.npart, w.newid, T);
+    CK(cudaGetLastError());
+    ctx->stats.launches += 2;
+    return GT_OK;
+}
+
+int upload_tables(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
+    auto up = [&](void* dst, const void* src, size_t bytes) -> int {
+        if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        return GT_OK;
+    };
+    int rc;
+    if ((rc = up(w.char_tab, P.char_tab.data(), sizeof(float) * P.char_tab.size()))) return rc;
+    if ((rc = up(w.gchar_tab, P.gchar_tab.data(), sizeof(float) * P.gchar_tab.size()))) return rc;
+    if ((rc = up(w.char_off, P.char_off.data(), sizeof(int) * P.char_off.size()))) return rc;
+    if ((rc = up(w.sig_off, P.sig_off.data(), sizeof(int) * P.sig_off.size()))) return rc;
+    if ((rc = up(w.bg_off, P.bg_off.data(), sizeof(int) * P.bg_off.size()))) return rc;
+    return GT_OK;
+}
+
+MovieBufs movie_bufs(const Plan& P, const Work& w, const void* frames) {
+    MovieBufs b{};
+    b.frames = frames;
+    b.T = P.T;
+    b.cap_c = P.cap_c; b.cap_p = P.cap_p; b.cap_m = P.cap_m; b.cap_e = P.cap_e;
+    b.cand = w.cand; b.fcount = w.fcount; b.rowcnt = w.rowcnt; b.pend = w.pend; b.npend = w.npend;
+    b.py = w.py; b.px = w.px; b.pm = w.pm; b.prec = w.prec; b.npart = w.npart;
+    b.G = P.G; b.ncx = P.ncx; b.ncy = P.ncy; b.gstart = w.gstart; b.gidx = w.gidx;
+    b.cperm = w.cperm; b.cy = w.cy; b.cx = w.cx; b.cm = w.cm; b.crec = w.crec; b.ccell = w.ccell;
+    b.cstart = w.cstart; b.cidx = w.cidx;
+    b.char_tab = w.char_tab; b.char_off = w.char_off; b.gchar_tab = w.gchar_tab;
+    b.err = w.err;
+    return b;
+}
+
+// The whole locate(+link) pipeline on device frames; table left in w.out.
+int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames, cudaStream_t st,
+                 int* err_bits, int64_t* nrows) {
+    const int T = P.T;
+    MovieBufs b = movie_bufs(P, w, d_frames);
+    int rc = upload_tables(ctx, P, w, st);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(w.fcount, 0, sizeof(int) * T, st));
+    CK(cudaMemsetAsync(w.npend, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(w.err, 0, sizeof(int) * 4, st));
+    CK(cudaFuncSetAttribute(locate_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_loc));
+    for (int i = 0; i < 5; ++i)
+        if (!ctx->ev[i]) CK(cudaEventCreate(&ctx->ev[i]));
+    CK(cudaEventRecord(ctx->ev[0], st));
+    const int ntiles = P.lp.ntx * P.lp.nty;
+    for (int f0 = 0; f0 < T; f0 += 65535) {
+        dim3 grid(ntiles, std::min(65535, T - f0));
+        locate_tiles_kernel<<<grid, 256, P.smem_loc, st>>>(P.lp, b, f0);
+        ctx->stats.launches += 1;
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[1], st));
+    CK(cudaFuncSetAttribute(fallback_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_fb));
+    fallback_walk_kernel<<<ctx->num_sms * 4, 128, P.smem_fb, st>>>(P.lp, b, P.fb_win);
+    CK(cudaGetLastError());
+    CK(cudaFuncSetAttribute(finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_fin));
+    finalize_kernel<<<T, 512, P.smem_fin, st>>>(P.lp, b, P.sep, P.link);
+    CK(cudaGetLastError());
+    scan_frames_kernel<<<1, 1024, 0, st>>>(w.npart, w.off, T);
+    CK(cudaGetLastError());
+    ctx->stats.launches += 3;
+    CK(cudaEventRecord(ctx->ev[2], st));
+    if (P.link) {
+        rc = run_link(ctx, P, w, st);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(ctx->ev[3], st));
+    AsmArgs a{};
+    a.T = T; a.H = P.H; a.W = P.W; a.cap_p = P.cap_p; a.cap_c = P.cap_c; a.ncols = (int)P.names.size();
+    a.has_link = P.link; a.cpu_processed = P.r.cpu_processed; a.characterize = P.r.characterize;
+    a.sig = P.r.has_sig; a.bg = P.r.has_bg;
+    a.frames = d_frames; a.dtype = P.dtype;
+    a.py = w.py; a.px = w.px; a.pm = w.pm; a.prec = w.prec; a.npart = w.npart; a.off = w.off;
+    a.cand = w.cand; a.root = w.root; a.newid = w.newid;
+    a.sig_off = w.sig_off; a.n_sig = (int)P.sig_off.size() / 2;
+    a.bg_off = w.bg_off; a.n_bg = (int)P.bg_off.size() / 2;
+    a.out = w.out;
+    assemble_kernel<<<T, 256, 0, st>>>(a);
+    CK(cudaGetLastError());
+    ctx->stats.launches += 1;
+    CK(cudaEventRecord(ctx->ev[4], st));
+    int hb[5];
+    CK(cudaMemcpyAsync(hb, w.err, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hb + 4, w.off + T, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int np = 0;
+    CK(cudaMemcpyAsync(&np, w.npend, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int nc_total = 0;
+    CK(cudaStreamSynchronize(st));
+    {
+        std::vector<int> fc(T);
+        CK(cudaMemcpy(fc.data(), w.fcount, sizeof(int) * T, cudaMemcpyDeviceToHost));
+        for (int v : fc) nc_total += v;
+    }
+    *err_bits = hb[0];
+    *nrows = hb[4];
+    ctx->stats.fallback_walks = np;
+    ctx->stats.particles = hb[4];
+    ctx->stats.candidates = nc_total;
+    cudaEventElapsedTime(&ctx->stats.ms_locate, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&ctx->stats.ms_finalize, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&ctx->stats.ms_link, ctx->ev[2], ctx->ev[3]);
+    cudaEventElapsedTime(&ctx->stats.ms_assemble, ctx->ev[3], ctx->ev[4]);
+    cudaEventElapsedTime(&ctx->stats.ms_total, ctx->ev[0], ctx->ev[4]);
+    return GT_OK;
+}
+
+int err_status(gt_ctx* ctx, int bits, bool* retry) {
+    *retry = false;
+    if (bits & ERR_SUBNET_BUDGET) {
+        ctx->err = "a linking subnetwork exceeded the search budget";
+        return GT_ERR_SUBNET_BUDGET;
+    }
+    if (bits & (ERR_CAND_OVERFLOW | ERR_PART_OVERFLOW | ERR_EDGE_OVERFLOW | ERR_MEM_OVERFLOW |
+                ERR_SCRATCH_OVERFLOW)) {
+        *retry = true;
+        ctx->err = "per-frame capacity exceeded (bits " + std::to_string(bits) + ")";
+        return GT_ERR_CAPACITY;
+    }
+    return GT_OK;
+}
+
+size_t elem_size(int dtype) { return dtype == GT_U16 ? 2 : 4; }
+
+int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, int H, int W,
+                 const gt_params* params, gt_table* out_tab, float* d_out, int64_t out_rows,
+                 int64_t* nrows_out, cudaStream_t st) {
+    if (!ctx) return GT_ERR_ARG;
+    ctx->err.clear();
+    ctx->stats = gt_stats{};
+    if (!frames || !params || T < 1 || H < 1 || W < 1 || (dtype != GT_U16 && dtype != GT_F32)) {
+        ctx->err = "invalid frames/shape/dtype";
+        return GT_ERR_ARG;
+    }
+    if ((long long)H * W > (1LL << 28)) { ctx->err = "frame too large"; return GT_ERR_ARG; }
+    Resolved r;
+    int rc = resolve(params, &r, &ctx->err);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    for (int scale = 1; scale <= 64; scale *= 4) {
+        Plan P;
+        rc = make_plan(r, T, H, W, dtype, scale, ctx->num_sms, &P, &ctx->err);
+        if (rc) return rc;
+        const size_t fbytes = host ? (size_t)T * H * W * elem_size(dtype) : 0;
+        Work w{};
+        const size_t need = carve(P, nullptr, &w, fbytes, true);
+        rc = ensure_arena(ctx, need);
+        if (rc) return rc;
+        carve(P, ctx->arena, &w, fbytes, true);
+        const void* dfr = frames;
+        if (host) {
+            CK(cudaMemcpyAsync(w.frames, frames, fbytes, cudaMemcpyHostToDevice, st));
+            dfr = w.frames;
+        }
+        int bits = 0;
+        int64_t nrows = 0;
+        rc = run_pipeline(ctx, P, w, dfr, st, &bits, &nrows);
+        if (rc) return rc;
+        bool retry;
+        rc = err_status(ctx, bits, &retry);
+        ctx->stats.retries = scale > 1 ? (int)std::log2((double)scale) / 2 : 0;
+        if (rc && retry && scale < 64) continue;
+        if (rc) return rc;
+        const int ncols = (int)P.names.size();
+        if (out_tab) {
+            out_tab->nrows = nrows;
+            out_tab->ncols = ncols;
+            std::memset(out_tab->names, 0, sizeof(out_tab->names));
+            std::memset(out_tab->types, 0, sizeof(out_tab->types));
+            for (int i = 0; i < ncols && i < GT_MAX_COLS; ++i) {
+                std::snprintf(out_tab->names[i], sizeof(out_tab->names[i]), "%s", P.names[i].c_str());
+                std::snprintf(out_tab->types[i], sizeof(out_tab->types[i]), "%s", P.types[i].c_str());
+            }
+            out_tab->data = (float*)std::malloc(sizeof(float) * (size_t)std::max<int64_t>(1, nrows) * ncols);
+            if (!out_tab->data) { ctx->err = "host allocation failed"; return GT_ERR_OOM; }
+            if (nrows > 0) {
+                CK(cudaMemcpyAsync(out_tab->data, w.out, sizeof(float) * (size_t)nrows * ncols,
+                                   cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+            }
+        }
+        if (d_out) {
+            const int64_t n = std::min(nrows, out_rows);
+            if (n > 0)
+                CK(cudaMemcpyAsync(d_out, w.out, sizeof(float) * (size_t)n * ncols, cudaMemcpyDeviceToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        if (nrows_out) *nrows_out = nrows;
+        return GT_OK;
+    }
+    return GT_ERR_CAPACITY;
+}
+
+}  // namespace
+
+namespace {
+thread_local std::string g_noctx_err;  // errors of calls made without a context
+}
+
+extern "C" {
+
+const char* gt_version(void) { return "gt-b200 0.1.0 (sm_100a)"; }
+
+int gt_ctx_create(int device, gt_ctx** out) {
+    if (!out) return GT_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return GT_ERR_CUDA;
+    gt_ctx* c = new gt_ctx();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return GT_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return GT_ERR_CUDA; }
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    *out = c;
+    return GT_OK;
+}
+
+void gt_ctx_destroy(gt_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->arena) cudaFree(ctx->arena);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* gt_last_error(const gt_ctx* ctx) { return ctx ? ctx->err.c_str() : g_noctx_err.c_str(); }
+
+int gt_column_names(const gt_params* params, char* buf, size_t buflen) {
+    if (!params || !buf) return -GT_ERR_ARG;
+    Resolved r;
+    int rc = resolve(params, &r, &g_noctx_err);
+    if (rc) return -rc;
+    std::vector<std::string> names, types;
+    column_list(r, names, types);
+    std::string s;
+    for (size_t i = 0; i < names.size(); ++i) {
+        if (i) s += ",";
+        s += names[i] + ":" + types[i];
+    }
+    if (s.size() + 1 > buflen) return -GT_ERR_ARG;
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return (int)names.size();
+}
+
+int gt_batch(gt_ctx* ctx, const void* frames, int dtype, int T, int H, int W, const gt_params* params,
+             gt_table* out) {
+    if (!out) return GT_ERR_ARG;
+    out->data = nullptr;
+    out->nrows = 0;
+    out->ncols = 0;
+    return batch_common(ctx, frames, true, dtype, T, H, W, params, out, nullptr, 0, nullptr,
+                        ctx ? ctx->stream : nullptr);
+}
+
+int gt_batch_device(gt_ctx* ctx, const void* d_frames, int dtype, int T, int H, int W,
+                    const gt_params* params, float* d_out, int64_t out_rows, int64_t* nrows, void* stream) {
+    cudaStream_t st = stream ? (cudaStream_t)stream : (ctx ? ctx->stream : nullptr);
+    return batch_common(ctx, d_frames, false, dtype, T, H, W, params, nullptr, d_out, out_rows, nrows, st);
+}
+
+void gt_table_free(gt_table* table) {
+    if (table && table->data) { std::free(table->data); table->data = nullptr; }
+}
+
+int gt_last_stats(const gt_ctx* ctx, gt_stats* out) {
+    if (!ctx || !out) return GT_ERR_ARG;
+    *out = ctx->stats;
+    return GT_OK;
+}
+
+int gt_link(gt_ctx* ctx, const float* rows, int64_t n, int ncols, float search_range, int has_memory,
+            uint32_t memory, uint64_t* ids) {
+    if (!ctx) return GT_ERR_ARG;
+    ctx->err.clear();
+    ctx->stats = gt_stats{};
+    if ((!rows && n > 0) || ncols < 4 || n < 0 || (n > 0 && !ids)) { ctx->err = "invalid table"; return GT_ERR_ARG; }
+    if (!(search_range > 0.0f && search_range < 4096.0f)) { ctx->err = "search_range must be in (0, 4096)"; return GT_ERR_ARG; }
+    if (n == 0) return GT_OK;
+    if (n > (1LL << 30)) { ctx->err = "table too large"; return GT_ERR_ARG; }
+    const uint32_t mem = has_memory ? memory : 0;
+    // FrameSubsetter (linking.rs:33-61): runs of equal column-0 values; the
+    // iterator starts with cur_frame = 0, so a first value != 0 yields a
+    // leading empty group.
+    std::vector<int64_t> gstart;
+    std::vector<int> gsize;
+    {
+        int64_t idx = 0;
+        float cur = 0.0f;
+        while (true) {
+            int64_t s = idx;
+            bool end = false;
+            while (true) {
+                if (idx >= n) { end = true; break; }
+                const float fr = rows[idx * ncols];
+                if (fr != cur) { cur = fr; break; }
+                ++idx;
+            }
+            if (end && idx == s) break;
+            gstart.push_back(s);
+            gsize.push_back((int)(idx - s));
+            if (end) break;
+        }
+    }
+    const int T = (int)gstart.size();
+    int maxg = 1;
+    float ymin = 0.f, ymax = 1.f, xmin = 0.f, xmax = 1.f;
+    bool first = true;
+    for (int64_t i = 0; i < n; ++i) {
+        const float y = rows[i * ncols + 2], x = rows[i * ncols + 3];
+        if (!std::isfinite(y) || !std::isfinite(x)) { ctx->err = "non-finite position"; return GT_ERR_ARG; }
+        if (first) { ymin = ymax = y; xmin = xmax = x; first = false; }
+        ymin = std::min(ymin, y); ymax = std::max(ymax, y);
+        xmin = std::min(xmin, x); xmax = std::max(xmax, x);
+    }
+    for (int g : gsize) maxg = std::max(maxg, g);
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    for (int scale = 1; scale <= 64; scale *= 4) {
+        Plan P;
+        P.T = T;
+        P.link = 1;
+        P.r = Resolved{};
+        P.r.has_search_range = 1;
+        P.r.search_range = search_range;
+        P.r.memory = mem;
+        P.cap_p = maxg;
+        P.cap_m = (int)std::max<long long>(1, (long long)mem * P.cap_p);
+        P.cap_s = P.cap_p + P.cap_m;
+        P.cap_e = (int)std::min<long long>((long long)P.cap_s * std::min(16 * scale, P.cap_p), 1LL << 30);
+        // grid over the positions' bounding box, shifted to start at 0
+        // cells of absolute positions; negative coordinates clamp into the
+        // first cell (clamping is monotone, so neighbours stay adjacent)
+        const double ext = std::max({(double)ymax, (double)xmax, 0.0}) + 1.0;
+        P.G = std::max({(int)std::ceil(search_range) + 1, 8, (int)std::ceil(ext / 128.0)});
+        P.ncy = (int)(std::max(ymax, 0.0f) / P.G) + 1;
+        P.ncx = (int)(std::max(xmax, 0.0f) / P.G) + 1;
+        (void)ymin; (void)xmin;
+        P.hsize = 2 * next_pow2(2LL * std::max({P.cap_p, P.cap_m, 32}));
+        const size_t nn = (size_t)P.cap_s + P.cap_p;
+        const size_t per_slot = 4 * (3 * (size_t)P.cap_s + 1) + 8 * (size_t)P.cap_e * 2 +
+                                4 * ((size_t)P.cap_p + 1) + 4 * 4 * nn + nn + 16 * nn + 4 + 8 * (size_t)P.hsize;
+        P.nslot = (int)std::max<size_t>(1, std::min<size_t>({(size_t)T, (size_t)ctx->num_sms * 4,
+                                                             ((size_t)6 << 30) / per_slot}));
+        P.cap_c = 1;
+        Work w{};
+        const size_t need = carve(P, nullptr, &w, 0, false);
+        int rc = ensure_arena(ctx, need);
+        if (rc) return rc;
+        carve(P, ctx->arena, &w, 0, false);
+        // particle slabs, positions shifted so the grid starts at the origin
+        std::vector<float> hy((size_t)T * P.cap_p, 0.f), hx((size_t)T * P.cap_p, 0.f);
+        for (int t = 0; t < T; ++t)
+            for (int i = 0; i < gsize[t]; ++i) {
+                const int64_t rr = gstart[t] + i;
+                hy[(size_t)t * P.cap_p + i] = rows[rr * ncols + 2];
+                hx[(size_t)t * P.cap_p + i] = rows[rr * ncols + 3];
+            }
+        CK(cudaMemcpyAsync(w.py, hy.data(), sizeof(float) * hy.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(w.px, hx.data(), sizeof(float) * hx.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(w.npart, gsize.data(), sizeof(int) * T, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(w.err, 0, sizeof(int) * 4, st));
+        CK(cudaFuncSetAttribute(grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(int) * (size_t)P.ncx * P.ncy)));
+        grid_kernel<<<T, 512, sizeof(int) * (size_t)P.ncx * P.ncy, st>>>(w.py, w.px, w.npart, P.cap_p, P.G,
+                                                                        P.ncy, P.ncx, w.gstart, w.gidx);
+        CK(cudaGetLastError());
+        scan_frames_kernel<<<1, 1024, 0, st>>>(w.npart, w.off, T);
+        rc = run_link(ctx, P, w, st);
+        if (rc) return rc;
+        // ids in row order: compact index g == row index
+        std::vector<int> root(n), newid(n);
+        CK(cudaMemcpyAsync(root.data(), w.root, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(newid.data(), w.newid, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+        int bits = 0;
+        CK(cudaMemcpyAsync(&bits, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        bool retry;
+        rc = err_status(ctx, bits, &retry);
+        if (rc && retry && scale < 64) continue;
+        if (rc) return rc;
+        for (int64_t i = 0; i < n; ++i) ids[i] = (uint64_t)newid[root[i]];
+        ctx->stats.particles = n;
+        return GT_OK;
+    }
+    return GT_ERR_CAPACITY;
+}
+
+}  // extern "C"

@@ -1,0 +1,513 @@
+// link.cu -- frame-to-frame linking on the device.
+//
+// Restates the reference linker (gpu-tracking/src/linking.rs:197-492):
+// candidate pairs closer than search_range (strict, squared distance),
+// connected components of the bipartite source/destination graph discovered
+// from each destination in index order, 1-1 components linked directly, and
+// every other component resolved by the reference's exhaustive
+// branch-and-bound (recurse2, linking.rs:390-452) with the same f32 score
+// arithmetic, option order (sources ascending, null last) and tie rule.
+//
+// Parallel structure.  Frame t's assignment depends only on the positions of
+// frames t-1 and t and on the memory entries M(t) (unlinked particles of the
+// previous `memory` frames, deduplicated by trajectory).  All frames are
+// linked at once for a guessed M; M is then recomputed from the result, and
+// only frames whose M changed are linked again, until M is a fixed point.
+// M(t) depends on frames < t only, so iteration k settles frame k at the
+// latest and the fixed point is the sequential result.
+#include "gt_device.cuh"
+
+namespace gt {
+
+
+
+namespace {
+constexpr int NTL = 256;
+
+__device__ __forceinline__ bool within_r(float qy, float qx, float iy, float ix, float r, float* dist) {
+    // kd-tree box pre-filter + linking.rs:91-100 distance (dest - source)
+    if (iy < qy - r || iy > qy + r) return false;
+    if (ix < qx - r || ix > qx + r) return false;
+    const float dy = iy - qy, dx = ix - qx;
+    float dd = 0.f;
+    dd = dd + dy * dy;
+    dd = dd + dx * dx;
+    *dist = dd;
+    return dd < r * r;
+}
+
+__device__ __forceinline__ int cell_of(float y, float x, float G, int ncy, int ncx) {
+    int cy = (int)floorf(y / G), cx = (int)floorf(x / G);
+    cy = clampi(cy, 0, ncy - 1);
+    cx = clampi(cx, 0, ncx - 1);
+    return cy * ncx + cx;
+}
+
+__device__ int uf_find(int* uf, int x) {
+    while (true) {
+        int p = uf[x];
+        if (p == x) return x;
+        int gp = uf[p];
+        if (gp != p) atomicCAS(&uf[x], p, gp);  // path halving
+        x = p;
+    }
+}
+
+__device__ void uf_union(int* uf, int a, int b) {
+    while (true) {
+        a = uf_find(uf, a);
+        b = uf_find(uf, b);
+        if (a == b) return;
+        if (a < b) { int t = a; a = b; b = t; }
+        if (atomicCAS(&uf[a], a, b) == a) return;
+    }
+}
+
+__device__ int block_scan_inplace_l(int* data, int n, int* warp_tot, int* s_total) {
+    const int chunk = (n + NTL - 1) / NTL;
+    const int q0 = threadIdx.x * chunk, q1 = min(q0 + chunk, n);
+    int mine = 0;
+    for (int q = q0; q < q1; ++q) mine += data[q];
+    int pos = block_excl_scan<NTL>(mine, warp_tot, s_total);
+    for (int q = q0; q < q1; ++q) { int v = data[q]; data[q] = pos; pos += v; }
+    __syncthreads();
+    return *s_total;
+}
+
+// Exhaustive search of one subnet (linking.rs:390-452) by one thread.
+// dests: destination indices in DFS order; sources are chosen through the
+// per-destination lists d_src/d_w (ascending source index); null costs r^2.
+// Returns false when the option-trial budget is exhausted.
+__device__ bool solve_subnet(const LinkBufs& L, int slot, const int* dests, int nd, const int* d_off,
+                             const int* d_src, const float* d_w, unsigned char* used, int* oi,
+                             int* cur, int* best_choice, float null_cost) {
+    float score = 0.f, best = CUDART_INF_F;
+    long long trials = 0;
+    int l = 0;
+    oi[0] = 0;
+    bool after_child = false;
+    while (true) {
+        const int d = dests[l];
+        const int nopt = d_off[d + 1] - d_off[d] + 1;
+        if (after_child) {
+            // child returned: undo this level's option and advance
+            const int o = oi[l];
+            const float c = (o == nopt - 1) ? null_cost : d_w[d_off[d] + o];
+            if (o != nopt - 1) used[d_src[d_off[d] + o]] = 0;
+            score -= c;
+            oi[l] = o + 1;
+            after_child = false;
+            continue;
+        }
+        const int o = oi[l];
+        if (o >= nopt || score > best) {  // loop exhausted, or early return
+            if (l == 0) break;
+            --l;
+            after_child = true;
+            continue;
+        }
+        if (++trials > L.budget) return false;
+        const bool is_null = (o == nopt - 1);
+        const float c = is_null ? null_cost : d_w[d_off[d] + o];
+        score += c;
+        if (!is_null) {
+            const int s = d_src[d_off[d] + o];
+            if (used[s]) { score -= c; oi[l] = o + 1; continue; }
+            used[s] = 1;
+            cur[l] = s;
+        } else {
+            cur[l] = -1;
+        }
+        if (l == nd - 1) {
+            if (score < best) {
+                best = score;
+                for (int q = 0; q < nd; ++q) best_choice[q] = cur[q];
+            }
+            if (!is_null) used[cur[l]] = 0;
+            score -= c;
+            oi[l] = o + 1;
+        } else {
+            ++l;
+            oi[l] = 0;
+        }
+    }
+    return true;
+}
+}  // namespace
+
+// One CTA per frame (grid-stride); frame t >= 1 links P(t-1) + M(t) to P(t).
+__global__ void __launch_bounds__(NTL) link_frames_kernel(LinkBufs L, int only_dirty) {
+    __shared__ int warp_tot[NTL / 32];
+    __shared__ int s_total;
+    const int slot = blockIdx.x;
+    const int cap_s = L.cap_s, cap_p = L.cap_p;
+    float* sy = L.s_y + (size_t)slot * cap_s;
+    float* sx = L.s_x + (size_t)slot * cap_s;
+    int* sh = L.s_h + (size_t)slot * cap_s;
+    int* sdeg = L.s_deg + (size_t)slot * (cap_s + 1);
+    int* edst = L.e_dst + (size_t)slot * L.cap_e;
+    float* ew = L.e_w + (size_t)slot * L.cap_e;
+    int* dcnt = L.d_cnt + (size_t)slot * (cap_p + 1);
+    int* dsrc = L.d_src + (size_t)slot * L.cap_e;
+    float* dw = L.d_w + (size_t)slot * L.cap_e;
+    const int nn = cap_s + cap_p;
+    int* uf = L.uf + (size_t)slot * nn;
+    int* cnd = L.c_nd + (size_t)slot * nn;
+    int* cns = L.c_ns + (size_t)slot * nn;
+    int* cmin = L.c_min + (size_t)slot * nn;
+    unsigned char* vis = L.vis + (size_t)slot * nn;
+    int* work = L.work + (size_t)slot * 4 * nn;
+    int* bump = L.bump + slot;
+    const float r = L.r;
+    const float G = (float)L.G;
+    const int ncell = L.ncx * L.ncy;
+
+    for (int t = blockIdx.x; t < L.T; t += gridDim.x) {
+        if (only_dirty && !L.dirty[t]) continue;
+        const int nd = L.npart[t];
+        int* pred = L.pred + L.off[t];
+        if (t == 0) {
+            for (int i = threadIdx.x; i < nd; i += NTL) pred[i] = -1;
+            __syncthreads();
+        } else {
+            const int n1 = L.npart[t - 1];
+            const int nm = L.mcount[t];
+            const int ns = n1 + nm;
+            if (threadIdx.x == 0) *bump = 0;
+            // sources: P(t-1) then M(t) (linking.rs:244-259 order)
+            for (int s = threadIdx.x; s < ns; s += NTL) {
+                int h;
+                if (s < n1) h = (t - 1) * cap_p + s;
+                else h = L.mlist[(size_t)t * L.cap_m + (s - n1)];
+                sh[s] = h;
+                sy[s] = L.py[h];
+                sx[s] = L.px[h];
+            }
+            for (int s = threadIdx.x; s < n1; s += NTL) L.lnext[(size_t)(t - 1) * cap_p + s] = 0;
+            __syncthreads();
+            const int* gs = L.gstart + (size_t)t * (ncell + 1);
+            const int* gi = L.gidx + (size_t)t * cap_p;
+            const float* dy = L.py + (size_t)t * cap_p;
+            const float* dx = L.px + (size_t)t * cap_p;
+            // candidate pairs: degree pass
+            for (int s = threadIdx.x; s < ns; s += NTL) {
+                const float qy = sy[s], qx = sx[s];
+                const int c = cell_of(qy, qx, G, L.ncy, L.ncx);
+                const int cy0 = c / L.ncx, cx0 = c - cy0 * L.ncx;
+                int deg = 0;
+                for (int ddy = -1; ddy <= 1; ++ddy) {
+                    const int yy = cy0 + ddy;
+                    if (yy < 0 || yy >= L.ncy) continue;
+                    for (int ddx = -1; ddx <= 1; ++ddx) {
+                        const int xx = cx0 + ddx;
+                        if (xx < 0 || xx >= L.ncx) continue;
+                        const int cc = yy * L.ncx + xx;
+                        for (int k = gs[cc]; k < gs[cc + 1]; ++k) {
+                            const int d = gi[k];
+                            float dist;
+                            if (within_r(qy, qx, dy[d], dx[d], r, &dist)) ++deg;
+                        }
+                    }
+                }
+                sdeg[s] = deg;
+            }
+            __syncthreads();
+            const int ne = block_scan_inplace_l(sdeg, ns, warp_tot, &s_total);
+            if (threadIdx.x == 0) sdeg[ns] = ne;
+            if (ne > L.cap_e) {
+                if (threadIdx.x == 0) atomicOr(L.err, ERR_EDGE_OVERFLOW);
+                for (int i = threadIdx.x; i < nd; i += NTL) pred[i] = -1;
+                __syncthreads();
+                continue;
+            }
+            for (int i = threadIdx.x; i <= nd; i += NTL) dcnt[i] = 0;
+            __syncthreads();
+            // fill, then order each source's list by destination index
+            for (int s = threadIdx.x; s < ns; s += NTL) {
+                const float qy = sy[s], qx = sx[s];
+                const int c = cell_of(qy, qx, G, L.ncy, L.ncx);
+                const int cy0 = c / L.ncx, cx0 = c - cy0 * L.ncx;
+                int w = sdeg[s];
+                const int w0 = w;
+                for (int ddy = -1; ddy <= 1; ++ddy) {
+                    const int yy = cy0 + ddy;
+                    if (yy < 0 || yy >= L.ncy) continue;
+                    for (int ddx = -1; ddx <= 1; ++ddx) {
+                        const int xx = cx0 + ddx;
+                        if (xx < 0 || xx >= L.ncx) continue;
+                        const int cc = yy * L.ncx + xx;
+                        for (int k = gs[cc]; k < gs[cc + 1]; ++k) {
+                            const int d = gi[k];
+                            float dist;
+                            if (within_r(qy, qx, dy[d], dx[d], r, &dist)) {
+                                int q = w++;
+                                while (q > w0 && edst[q - 1] > d) { edst[q] = edst[q - 1]; ew[q] = ew[q - 1]; --q; }
+                                edst[q] = d; ew[q] = dist;
+                                atomicAdd(&dcnt[d], 1);
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            block_scan_inplace_l(dcnt, nd + 1, warp_tot, &s_total);
+            // destination lists, ascending source index (linking.rs:310-315)
+            int* dcur = cmin;  // reuse: cursors per destination
+            for (int d = threadIdx.x; d < nd; d += NTL) dcur[d] = dcnt[d];
+            __syncthreads();
+            for (int s = threadIdx.x; s < ns; s += NTL) {
+                for (int q = sdeg[s]; q < sdeg[s + 1]; ++q) {
+                    const int d = edst[q];
+                    const int k = atomicAdd(&dcur[d], 1);
+                    dsrc[k] = s;
+                    dw[k] = ew[q];
+                }
+            }
+            __syncthreads();
+            for (int d = threadIdx.x; d < nd; d += NTL) {
+                const int a = dcnt[d], e = dcnt[d + 1];
+                for (int q = a + 1; q < e; ++q) {
+                    const int ks = dsrc[q];
+                    const float kw = dw[q];
+                    int z = q;
+                    while (z > a && dsrc[z - 1] > ks) { dsrc[z] = dsrc[z - 1]; dw[z] = dw[z - 1]; --z; }
+                    dsrc[z] = ks; dw[z] = kw;
+                }
+            }
+            // union-find over sources [0, ns) and destinations [ns, ns + nd)
+            const int nnode = ns + nd;
+            for (int i = threadIdx.x; i < nnode; i += NTL) {
+                uf[i] = i; cnd[i] = 0; cns[i] = 0; vis[i] = 0;
+            }
+            __syncthreads();
+            for (int s = threadIdx.x; s < ns; s += NTL)
+                for (int q = sdeg[s]; q < sdeg[s + 1]; ++q) uf_union(uf, s, ns + edst[q]);
+            __syncthreads();
+            for (int i = threadIdx.x; i < nnode; i += NTL) uf[i] = uf_find(uf, i);
+            __syncthreads();
+            for (int i = threadIdx.x; i < nnode; i += NTL) cmin[i] = 0x7fffffff;
+            __syncthreads();
+            for (int s = threadIdx.x; s < ns; s += NTL)
+                if (sdeg[s + 1] > sdeg[s]) atomicAdd(&cns[uf[s]], 1);
+            for (int d = threadIdx.x; d < nd; d += NTL) {
+                const int rt = uf[ns + d];
+                atomicAdd(&cnd[rt], 1);
+                atomicMin(&cmin[rt], d);
+            }
+            __syncthreads();
+            // components, each resolved by the thread of its first destination
+            const float null_cost = r * r;
+            for (int d = threadIdx.x; d < nd; d += NTL) {
+                const int rt = uf[ns + d];
+                if (cmin[rt] != d) continue;
+                const int cd = cnd[rt], cs = cns[rt];
+                if (cd == 1 && cs == 0) { pred[d] = -1; continue; }
+                if (cd == 1 && cs == 1) {
+                    const int s = dsrc[dcnt[d]];
+                    const int h = sh[s];
+                    pred[d] = L.off[h / cap_p] + (h % cap_p);
+                    if (s < n1) L.lnext[(size_t)(t - 1) * cap_p + s] = 1;
+                    continue;
+                }
+                // subnet: DFS preorder from d (linking.rs:316-342)
+                const int sz = cd + cs;
+                const int base = atomicAdd(bump, 4 * sz);
+                int* stk_n = work + base;          // node ids (dest: ns + d)
+                int* stk_p = stk_n + sz;           // next neighbour position
+                int* path = stk_p + sz;            // destinations in DFS order
+                int* choice = path + sz;           // per level: cur | best
+                int top = 0, npath = 0;
+                stk_n[0] = ns + d; stk_p[0] = 0; vis[ns + d] = 1; path[npath++] = d;
+                top = 1;
+                while (top > 0) {
+                    const int node = stk_n[top - 1];
+                    int pos = stk_p[top - 1];
+                    int next = -1;
+                    if (node >= ns) {
+                        const int dd2 = node - ns;
+                        if (dcnt[dd2] + pos < dcnt[dd2 + 1]) next = dsrc[dcnt[dd2] + pos];
+                    } else {
+                        if (sdeg[node] + pos < sdeg[node + 1]) next = ns + edst[sdeg[node] + pos];
+                    }
+                    if (next < 0) { --top; continue; }
+                    stk_p[top - 1] = pos + 1;
+                    if (vis[next]) continue;
+                    vis[next] = 1;
+                    if (next >= ns) path[npath++] = next - ns;
+                    stk_n[top] = next; stk_p[top] = 0; ++top;
+                }
+                // branch and bound; `vis` bytes of sources double as `used`
+                // flags: reset them first (all sources of the subnet were
+                // visited above)
+                for (int q = 0; q < npath; ++q) {
+                    const int dd2 = path[q];
+                    for (int z = dcnt[dd2]; z < dcnt[dd2 + 1]; ++z) vis[dsrc[z]] = 0;
+                }
+                int* oi = stk_n;                     // reuse the DFS stack
+                int* cur = stk_p;
+                int* bestc = choice;
+                for (int q = 0; q < npath; ++q) bestc[q] = -1;
+                const bool ok = solve_subnet(L, slot, path, npath, dcnt, dsrc, dw, vis, oi, cur, bestc,
+                                             null_cost);
+                if (!ok) atomicOr(L.err, ERR_SUBNET_BUDGET);
+                for (int q = 0; q < npath; ++q) {
+                    const int s = bestc[q];
+                    if (s < 0) { pred[path[q]] = -1; continue; }
+                    const int h = sh[s];
+                    pred[path[q]] = L.off[h / cap_p] + (h % cap_p);
+                    if (s < n1) L.lnext[(size_t)(t - 1) * cap_p + s] = 1;
+                }
+            }
+            __syncthreads();
+        }
+        // rank of each new particle within the frame (linking.rs:470)
+        int* nr = L.newrank + L.off[t];
+        const int chunk = (nd + NTL - 1) / NTL;
+        const int q0 = threadIdx.x * chunk, q1 = min(q0 + chunk, nd);
+        int mine = 0;
+        for (int q = q0; q < q1; ++q) mine += (pred[q] < 0);
+        int pos = block_excl_scan<NTL>(mine, warp_tot, &s_total);
+        for (int q = q0; q < q1; ++q) nr[q] = pred[q] < 0 ? pos++ : -1;
+        if (threadIdx.x == 0) L.newcount[t] = s_total;
+        __syncthreads();
+    }
+}
+
+// Memory entries M(t) (linking.rs:244-259): particles of frames
+// [t-1-memory, t-2] that the next frame did not link (the `unused` lists of
+// linking.rs:479-485, oldest list first, index order within a list),
+// skipping trajectories present in frame t-1 and keeping the first entry of
+// each trajectory.  Marks frames whose M changed.
+__global__ void __launch_bounds__(NTL) memory_kernel(LinkBufs L, int memory) {
+    __shared__ int warp_tot[NTL / 32];
+    __shared__ int s_total;
+    __shared__ int s_diff;
+    const int slot = blockIdx.x;
+    const int cap_p = L.cap_p;
+    const int nn = L.cap_s + cap_p;
+    int* ch = L.work + (size_t)slot * 4 * nn;    // candidate slab handles
+    int* cr = ch + nn;                            // candidate roots
+    int* cpos = cr + nn;                          // scan workspace
+    int* hk = L.hkey + (size_t)slot * L.hsize;
+    int* hv = L.hval + (size_t)slot * L.hsize;
+    for (int t = blockIdx.x; t < L.T; t += gridDim.x) {
+        const int fbeg = max(0, t - 1 - memory), fend = t - 2;
+        if (fend < fbeg) continue;
+        // candidates in (frame, index) order
+        int nc = 0;
+        for (int f = fbeg; f <= fend; ++f) {
+            const int n = L.npart[f];
+            const unsigned char* ln = L.lnext + (size_t)f * cap_p;
+            for (int i = threadIdx.x; i < n; i += NTL) cpos[i] = ln[i] ? 0 : 1;
+            __syncthreads();
+            const int k = block_scan_inplace_l(cpos, n, warp_tot, &s_total);
+            for (int i = threadIdx.x; i < n; i += NTL) {
+                if (ln[i]) continue;
+                const int j = nc + cpos[i];
+                if (j < nn) {
+                    ch[j] = f * cap_p + i;
+                    cr[j] = L.root[L.off[f] + i];
+                }
+            }
+            nc += k;
+            __syncthreads();
+        }
+        if (nc > nn) { if (threadIdx.x == 0) atomicOr(L.err, ERR_MEM_OVERFLOW); nc = nn; }
+        const int n1 = L.npart[t - 1];
+        int hs1 = 64;
+        while (hs1 < 2 * n1) hs1 <<= 1;
+        int hs2 = 64;
+        while (hs2 < 2 * nc) hs2 <<= 1;
+        if (hs1 + hs2 > L.hsize) { if (threadIdx.x == 0) atomicOr(L.err, ERR_SCRATCH_OVERFLOW); continue; }
+        int* k1 = hk;
+        int* k2 = hk + hs1;
+        int* v2 = hv + hs1;
+        for (int i = threadIdx.x; i < hs1 + hs2; i += NTL) { hk[i] = -1; hv[i] = 0x7fffffff; }
+        __syncthreads();
+        // trajectories present in frame t-1
+        for (int i = threadIdx.x; i < n1; i += NTL) {
+            const int key = L.root[L.off[t - 1] + i];
+            unsigned hsh = ((unsigned)key * 2654435761u) & (hs1 - 1);
+            while (true) {
+                const int prev = atomicCAS(&k1[hsh], -1, key);
+                if (prev == -1 || prev == key) break;
+                hsh = (hsh + 1) & (hs1 - 1);
+            }
+        }
+        // first candidate of each trajectory
+        for (int j = threadIdx.x; j < nc; j += NTL) {
+            const int key = cr[j];
+            unsigned hsh = ((unsigned)key * 2654435761u) & (hs2 - 1);
+            while (true) {
+                const int prev = atomicCAS(&k2[hsh], -1, key);
+                if (prev == -1 || prev == key) break;
+                hsh = (hsh + 1) & (hs2 - 1);
+            }
+            atomicMin(&v2[hsh], j);
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < nc; j += NTL) {
+            const int key = cr[j];
+            bool keep = true;
+            unsigned hsh = ((unsigned)key * 2654435761u) & (hs1 - 1);
+            while (true) {
+                const int kk = k1[hsh];
+                if (kk == -1) break;
+                if (kk == key) { keep = false; break; }
+                hsh = (hsh + 1) & (hs1 - 1);
+            }
+            if (keep) {
+                hsh = ((unsigned)key * 2654435761u) & (hs2 - 1);
+                while (k2[hsh] != key) hsh = (hsh + 1) & (hs2 - 1);
+                keep = v2[hsh] == j;
+            }
+            cpos[j] = keep ? 1 : 0;
+        }
+        if (threadIdx.x == 0) s_diff = 0;
+        __syncthreads();
+        const int nk = block_scan_inplace_l(cpos, nc, warp_tot, &s_total);
+        int* ml = L.mlist + (size_t)t * L.cap_m;
+        const int old = L.mcount[t];
+        if (nk > L.cap_m) { if (threadIdx.x == 0) atomicOr(L.err, ERR_MEM_OVERFLOW); continue; }
+        if (old != nk && threadIdx.x == 0) s_diff = 1;
+        __syncthreads();
+        for (int j = threadIdx.x; j < nc; j += NTL) {
+            const int a = cpos[j];
+            const int nxt = (j + 1 < nc) ? cpos[j + 1] : nk;
+            if (nxt > a && ml[a] != ch[j]) s_diff = 1;
+        }
+        __syncthreads();
+        if (s_diff) {
+            for (int j = threadIdx.x; j < nc; j += NTL) {
+                const int a = cpos[j];
+                const int nxt = (j + 1 < nc) ? cpos[j + 1] : nk;
+                if (nxt > a) ml[a] = ch[j];
+            }
+            if (threadIdx.x == 0) {
+                L.mcount[t] = nk;
+                L.dirty[t] = 1;
+                atomicAdd(L.ndirty, 1);
+            }
+        } else if (threadIdx.x == 0) {
+            L.dirty[t] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+// Trajectory roots by pointer jumping over `pred` (compact indices).
+__global__ void root_init_kernel(LinkBufs L, const int* total) {
+    const int n = *total;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const int p = L.pred[g];
+        L.root[g] = p < 0 ? g : p;
+    }
+}
+
+__global__ void root_jump_kernel(LinkBufs L, const int* total) {
+    const int n = *total;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x)
+        L.root[g] = L.root[L.root[g]];
+}
+
+}  // namespace gt

@@ -1,0 +1,98 @@
+"""Module-level functions of the reference's pyo3 module `gpu_tracking`
+(gpu-tracking/src/lib.rs:44-236), backed by libgt.so on a B200.
+
+Same names, positional order and defaults:
+  batch_rust(pyarr, diameter, minmass, maxsize, separation, noise_size,
+             smoothing_size, threshold, invert, percentile, topn, preprocess,
+             max_iterations, characterize, filter_close, search_range, memory,
+             cpu_processed, sig_radius, bg_radius, gap_radius)
+      -> (float32 array [rows, cols], [(name, type), ...])
+  link_rust(pyarr, search_range, memory=None) -> uint64 array
+The reference accepts float32 frames only (lib.rs:50); uint16 frames are
+accepted as well.  Unsupported options raise NotImplementedError as the
+reference's `not_implemented!` does (lib.rs:28-39, 73-74).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native
+
+PARAM_ORDER = ["minmass", "maxsize", "separation", "noise_size", "smoothing_size", "threshold", "invert",
+               "percentile", "topn", "preprocess", "max_iterations", "characterize", "filter_close",
+               "search_range", "memory", "cpu_processed", "sig_radius", "bg_radius", "gap_radius"]
+
+
+def _frames_array(pyarr):
+    arr = np.asarray(pyarr)
+    if arr.ndim != 3:
+        raise ValueError(f"expected a (frames, rows, cols) array, got shape {arr.shape}")
+    if arr.dtype == np.uint16:
+        dtype = _native.GT_U16
+    elif arr.dtype == np.float32:
+        dtype = _native.GT_F32
+    else:
+        raise TypeError(f"frames must be float32 or uint16, got {arr.dtype}")
+    if not arr.flags["C_CONTIGUOUS"]:
+        # execute_gpu.rs:497-499 rejects non-standard layouts
+        raise ValueError("Array is not standard layout")
+    return arr, dtype
+
+
+def batch_rust(pyarr, diameter, minmass=None, maxsize=None, separation=None, noise_size=None,
+               smoothing_size=None, threshold=None, invert=None, percentile=None, topn=None, preprocess=None,
+               max_iterations=None, characterize=None, filter_close=None, search_range=None, memory=None,
+               cpu_processed=None, sig_radius=None, bg_radius=None, gap_radius=None, device=0):
+    """Locate (and link when search_range is given) features in every frame."""
+    arr, dtype = _frames_array(pyarr)
+    vals = dict(minmass=minmass, maxsize=maxsize, separation=separation, noise_size=noise_size,
+                smoothing_size=smoothing_size, threshold=threshold, invert=invert, percentile=percentile,
+                topn=topn, preprocess=preprocess, max_iterations=max_iterations, characterize=characterize,
+                filter_close=filter_close, search_range=search_range, memory=memory,
+                cpu_processed=cpu_processed, sig_radius=sig_radius, bg_radius=bg_radius,
+                gap_radius=gap_radius)
+    params = _native.make_params(diameter, **vals)
+    lib = _native.load()
+    ctx = _native.context(device)
+    tab = _native.GtTable()
+    T, H, W = arr.shape
+    st = lib.gt_batch(ctx, arr.ctypes.data_as(ctypes.c_void_p), dtype, T, H, W, ctypes.byref(params),
+                      ctypes.byref(tab))
+    _native.check(st, ctx)
+    try:
+        n, c = tab.nrows, tab.ncols
+        out = np.ctypeslib.as_array(tab.data, shape=(max(n, 1) * c,))[: n * c].copy().reshape(n, c)
+        cols = [(tab.names[i].value.decode(), tab.types[i].value.decode()) for i in range(c)]
+    finally:
+        lib.gt_table_free(ctypes.byref(tab))
+    return out, cols
+
+
+def batch_file_rust(filename, diameter, channel=None, *args, **kwargs):
+    """File ingest (TIFF/ETS) is not part of this build's hot path."""
+    raise NotImplementedError("batch_file_rust: file ingest is not implemented in the B200 build")
+
+
+def link_rust(pyarr, search_range, memory=None, device=0):
+    """Link a (frame, mass, y, x, ...) float32 table; returns uint64 IDs."""
+    arr = np.ascontiguousarray(np.asarray(pyarr, dtype=np.float32))
+    if arr.ndim != 2 or arr.shape[1] < 4:
+        raise ValueError("expected an (n, >=4) float32 table")
+    lib = _native.load()
+    ctx = _native.context(device)
+    ids = np.empty(arr.shape[0], dtype=np.uint64)
+    st = lib.gt_link(ctx, arr.ctypes.data_as(ctypes.c_void_p), arr.shape[0], arr.shape[1], float(search_range),
+                     0 if memory is None else 1, 0 if memory is None else int(memory),
+                     ids.ctypes.data_as(ctypes.c_void_p))
+    _native.check(st, ctx)
+    return ids
+
+
+def column_names(diameter=9, **kw):
+    """execute_gpu.rs:197-226 column list for a parameter set."""
+    params = _native.make_params(diameter, **kw)
+    buf = ctypes.create_string_buffer(1024)
+    n = _native.load().gt_column_names(ctypes.byref(params), buf, 1024)
+    if n < 0:
+        _native.check(-n, None)
+    return [tuple(x.split(":")) for x in buf.value.decode().split(",")]
