@@ -167,6 +167,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--frames", type=int, default=None,
+                    help="smaller movie of the same spot model (profiling captures only)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -185,7 +188,7 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     spec, params = workload()
-    rspec = synth.scaled(spec, seed=spec.seed + rank)
+    rspec = synth.scaled(spec, frames=args.frames, seed=spec.seed + rank)
     movie = synth.make_movie(rspec)
     T, H, W = movie.shape
     lib = _native.load()
@@ -229,21 +232,23 @@ def main():
     value = world * T / (ms_max / 1e3)
 
     # end to end through the public API: pinned host frames in, table out
-    pinned = torch.from_numpy(movie).pin_memory() if hasattr(torch, "uint16") else None
-    host_in = pinned.numpy() if pinned is not None else movie
-    batch_rust(host_in, **params)
-    if world > 1:
-        dist.barrier()
-    e2e_steps = max(1, min(args.steps, 3))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        tab, cols = batch_rust(host_in, **params)
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    te = torch.tensor([e2e_s], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * T / float(te.item())
+    e2e_value, tab, pinned = None, None, None
+    if not args.no_e2e:
+        pinned = torch.from_numpy(movie).pin_memory()
+        host_in = pinned.numpy()
+        batch_rust(host_in, **params)
+        if world > 1:
+            dist.barrier()
+        e2e_steps = max(1, min(args.steps, 3))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            tab, cols = batch_rust(host_in, **params)
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        te = torch.tensor([e2e_s], device=f"cuda:{local}")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_value = world * T / float(te.item())
 
     if rank == 0:
         loc_ms = float(np.median([s["ms_locate"] for s in stats]))
@@ -274,11 +279,15 @@ def main():
             "link_iterations": stats[-1]["link_iterations"], "fallback_walks": stats[-1]["fallback_walks"],
             "candidates_per_frame": cands / T, "particles_per_frame": rows / T,
             "gpu_launches": int(sum(s["launches"] for s in stats)),
-            "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": int(movie.nbytes),
-                    "d2h_bytes_per_step": int(tab.nbytes), "timing": "host clock around synchronous calls",
-                    "pinned_input": pinned is not None},
+            "e2e": None if e2e_value is None else {
+                "value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": int(movie.nbytes),
+                "d2h_bytes_per_step": int(tab.nbytes), "timing": "host clock around synchronous calls",
+                "pinned_input": True},
             "clocks": clk.summary(),
         }
+        if args.frames is not None:
+            line["config"]["frames"] = T
+            line["config"]["workload"] = f"profiling capture: {T} frames of the same spot model"
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(movie, params)
         print(json.dumps(line), flush=True)
