@@ -10,6 +10,11 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <map>
+
 #include "gt.h"
 #include "gt_internal.cuh"
 
@@ -27,6 +32,11 @@ __global__ void newid_kernel(const int* newrank, const int* newbase, const int* 
 __global__ void assemble_kernel(AsmArgs a);
 __global__ void grid_kernel(const float* py, const float* px, const int* npart, int cap_p, int G,
                             int ncy, int ncx, int* gstart, int* gidx);
+bool fast_supported(int kr, int dd);
+cudaError_t launch_locate_fast(int kr, int dd, dim3 grid, cudaStream_t st, const LocParams& p,
+                               const MovieBufs& b, const FastGeo& g, const CUtensorMap& map, int frame0);
+cudaError_t launch_verify_division(float divisor, FixedDiv f, unsigned int* d_count, int num_sms,
+                                   cudaStream_t st);
 }  // namespace gt
 
 using namespace gt;
@@ -40,6 +50,9 @@ struct gt_ctx {
     gt_stats stats{};
     int num_sms = 148;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    std::map<uint32_t, bool> div_ok;  // divisor bits -> fast division verified exact
+    unsigned int* d_count = nullptr;
+    int force_generic = 0;            // testing hook: always use locate_tiles_kernel
 };
 
 namespace {
@@ -151,6 +164,8 @@ struct Plan {
     int nslot = 1, hsize = 64;
     size_t smem_loc = 0, smem_fb = 0, smem_fin = 0;
     int fb_win = 0;
+    int fast = 0;
+    FastGeo fg{};
     std::vector<float> char_tab, gchar_tab;
     std::vector<int> char_off, sig_off, bg_off;
     std::vector<std::string> names, types;
@@ -190,7 +205,7 @@ void annulus_inds_f(float outer, float inner, std::vector<int>& off) {
 }
 
 int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int num_sms, Plan* pl,
-              std::string* msg) {
+              std::string* msg, int force_generic_flag = 0) {
     Plan& P = *pl;
     P.T = T; P.H = H; P.W = W; P.dtype = dtype; P.r = r;
     LocParams& lp = P.lp;
@@ -221,6 +236,41 @@ int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int 
     lp.minmass = r.minmass;
     lp.hp = std::max({lp.o, lp.D - 1 - lp.o, lp.char_r, lp.rint_c + 2, 1});
     lp.TH = LOC_TH; lp.TW = LOC_TW;
+    P.fast = 0;
+    if (dtype == GT_U16 && fast_supported(lp.krad, lp.D) && lp.krad <= 7 && !force_generic_flag) {
+        FastGeo& g = P.fg;
+        std::memset(&g, 0, sizeof(g));
+        const int KR = lp.krad;
+        g.hp = lp.hp + ((lp.hp - lp.o) & 1);  // keep hp - offset even (row pairs)
+        g.L = (g.hp + KR + 7) / 8 * 8;
+        g.hx = g.L - KR;
+        g.RW = (g.L + 64 + g.hp + KR + 7) / 8 * 8;
+        g.RH = 64 + 2 * g.hp + 2 * KR;
+        g.PH = 64 + 2 * g.hp;
+        g.PW = g.RW - 2 * KR;
+        g.NPW = (g.PW + 7) / 8;
+        g.PWC = 8 * g.NPW;
+        g.NRQ = (g.PH + 7) / 8;
+        auto odd = [](int x) { return x | 1; };
+        g.RPS = odd(g.PWC + 2 * KR);
+        g.GPS = odd(g.PWC);
+        g.P2S = odd(g.PWC);
+        g.RMS = odd(64);
+        auto al = [](size_t x) { return (x + 127) / 128 * 128; };
+        const size_t u = al((size_t)g.RH * g.RW * 2);
+        const size_t rp = al(std::max((size_t)(g.RH / 2) * g.RPS * 8, (size_t)(4 * g.NRQ) * g.P2S * 8));
+        const size_t gpb = al(std::max({(size_t)(4 * g.NRQ + KR) * g.GPS * 8, (size_t)(g.PH / 2 + 1) * g.RMS * 8,
+                                        (size_t)64 * 64 * 4, (size_t)64 * 64 + 4 * 4 * 512}));
+        g.off_rp = (int)u;
+        g.off_gp = (int)(u + rp);
+        g.off_bp = (int)(u + rp + gpb);
+        g.smem = (int)(u + rp + 2 * gpb);
+        if (g.smem <= 227 * 1024 && g.RW <= 256 && g.RH <= 256) {
+            P.fast = 1;
+            lp.TH = 64;
+            lp.TW = 64;
+        }
+    }
     lp.ntx = (W + lp.TW - 1) / lp.TW;
     lp.nty = (H + lp.TH - 1) / lp.TH;
     lp.dtype = dtype;
@@ -492,6 +542,59 @@ MovieBufs movie_bufs(const Plan& P, const Work& w, const void* frames) {
     return b;
 }
 
+// Exhaustive check (cached per divisor) that the fixed-divisor division of
+// the fast kernel equals IEEE division for every positive binary32 dividend.
+int fast_division(gt_ctx* ctx, const Plan& P, FastGeo* g, cudaStream_t st) {
+    const float divs[2] = {P.lp.norm, P.lp.kk};
+    FixedDiv fdv[2];
+    bool all = true;
+    for (int i = 0; i < 2; ++i) {
+        const float b = divs[i];
+        fdv[i].y = 1.0f / b;
+        fdv[i].nb = -b;
+        uint32_t bits;
+        std::memcpy(&bits, &b, 4);
+        auto it = ctx->div_ok.find(bits);
+        if (it == ctx->div_ok.end()) {
+            if (!ctx->d_count) CK(cudaMalloc((void**)&ctx->d_count, sizeof(unsigned int)));
+            CK(cudaMemsetAsync(ctx->d_count, 0, sizeof(unsigned int), st));
+            CK(launch_verify_division(b, fdv[i], ctx->d_count, ctx->num_sms, st));
+            unsigned int bad = 0;
+            CK(cudaMemcpyAsync(&bad, ctx->d_count, sizeof(bad), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            it = ctx->div_ok.emplace(bits, bad == 0).first;
+        }
+        all = all && it->second;
+    }
+    g->fastdiv = all ? 1 : 0;
+    g->dnorm = fdv[0];
+    g->dkk = fdv[1];
+    return GT_OK;
+}
+
+// TMA descriptor over the movie (u16, dims W x H x T).  Needs a 16-byte
+// aligned base and a row pitch that is a multiple of 16 bytes.
+bool make_tensor_map(CUtensorMap* map, const void* frames, const Plan& P) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    if (((uintptr_t)frames & 15) || (P.W * 2) % 16) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)P.W, (cuuint64_t)P.H, (cuuint64_t)P.T};
+    cuuint64_t strides[2] = {(cuuint64_t)P.W * 2, (cuuint64_t)P.W * P.H * 2};
+    cuuint32_t box[3] = {(cuuint32_t)P.fg.RW, (cuuint32_t)P.fg.RH, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, const_cast<void*>(frames), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 // The whole locate(+link) pipeline on device frames; table left in w.out.
 int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames, cudaStream_t st,
                  int* err_bits, int64_t* nrows) {
@@ -505,12 +608,27 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
     CK(cudaFuncSetAttribute(locate_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_loc));
     for (int i = 0; i < 5; ++i)
         if (!ctx->ev[i]) CK(cudaEventCreate(&ctx->ev[i]));
-    CK(cudaEventRecord(ctx->ev[0], st));
     const int ntiles = P.lp.ntx * P.lp.nty;
-    for (int f0 = 0; f0 < T; f0 += 65535) {
-        dim3 grid(ntiles, std::min(65535, T - f0));
-        locate_tiles_kernel<<<grid, 256, P.smem_loc, st>>>(P.lp, b, f0);
-        ctx->stats.launches += 1;
+    if (P.fast) {
+        FastGeo g = P.fg;
+        rc = fast_division(ctx, P, &g, st);
+        if (rc) return rc;
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof(map));
+        g.use_tma = make_tensor_map(&map, d_frames, P) ? 1 : 0;
+        CK(cudaEventRecord(ctx->ev[0], st));
+        for (int f0 = 0; f0 < T; f0 += 65535) {
+            dim3 grid(ntiles, std::min(65535, T - f0));
+            CK(launch_locate_fast(P.lp.krad, P.lp.D, grid, st, P.lp, b, g, map, f0));
+            ctx->stats.launches += 1;
+        }
+    } else {
+        CK(cudaEventRecord(ctx->ev[0], st));
+        for (int f0 = 0; f0 < T; f0 += 65535) {
+            dim3 grid(ntiles, std::min(65535, T - f0));
+            locate_tiles_kernel<<<grid, 256, P.smem_loc, st>>>(P.lp, b, f0);
+            ctx->stats.launches += 1;
+        }
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], st));
@@ -570,6 +688,10 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
 
 int err_status(gt_ctx* ctx, int bits, bool* retry) {
     *retry = false;
+    if (bits & ERR_DEVICE_TIMEOUT) {
+        ctx->err = "a bounded device wait expired (TMA tile load)";
+        return GT_ERR_DEVICE_TIMEOUT;
+    }
     if (bits & ERR_SUBNET_BUDGET) {
         ctx->err = "a linking subnetwork exceeded the search budget";
         return GT_ERR_SUBNET_BUDGET;
@@ -602,7 +724,7 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
     CK(cudaSetDevice(ctx->device));
     for (int scale = 1; scale <= 64; scale *= 4) {
         Plan P;
-        rc = make_plan(r, T, H, W, dtype, scale, ctx->num_sms, &P, &ctx->err);
+        rc = make_plan(r, T, H, W, dtype, scale, ctx->num_sms, &P, &ctx->err, ctx->force_generic);
         if (rc) return rc;
         const size_t fbytes = host ? (size_t)T * H * W * elem_size(dtype) : 0;
         Work w{};
@@ -682,6 +804,7 @@ void gt_ctx_destroy(gt_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->arena) cudaFree(ctx->arena);
+    if (ctx->d_count) cudaFree(ctx->d_count);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -63,6 +63,30 @@ enum ErrBits {
     ERR_SUBNET_BUDGET = 8,
     ERR_MEM_OVERFLOW = 16,
     ERR_SCRATCH_OVERFLOW = 32,
+    ERR_DEVICE_TIMEOUT = 64,
+};
+
+// Division by a fixed divisor b: y = RN(1/b), nb = -b (see gt_simd.cuh).
+struct FixedDiv {
+    float y;
+    float nb;
+};
+
+// Geometry of the fast locate kernel (64 x 64 output tiles).
+struct FastGeo {
+    int hp;          // processed halo above/below the tile (hp - offset even)
+    int L;           // raw columns left of the tile (multiple of 8)
+    int hx;          // processed columns left of the tile (L - krad)
+    int RH, RW;      // raw region (u16 staging, RW multiple of 8)
+    int PH, PW;      // processed region
+    int NPW, PWC;    // 8-column chunks of the row pass, columns computed
+    int NRQ;         // 8-row chunks of the column pass
+    int RPS, GPS, P2S, RMS;  // odd row-pair strides (float2 units)
+    int off_rp, off_gp, off_bp;  // byte offsets of the regions
+    int smem;
+    int use_tma;
+    int fastdiv;
+    FixedDiv dnorm, dkk;
 };
 
 // Per-movie device buffers and capacities.
