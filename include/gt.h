@@ -129,6 +129,12 @@ GT_API int gt_link(gt_ctx* ctx, const float* rows, int64_t n, int ncols, float s
 /* Free a table returned by gt_batch. */
 GT_API void gt_table_free(gt_table* table);
 
+/* Tuning options of a context (no reference counterpart):
+ *   "locate_tile_rows"  output tile height of the specialised locate kernel, 32 or 64
+ *   "force_generic"     1 = always use the generic locate kernel
+ * Returns GT_ERR_ARG for an unknown key or value. */
+GT_API int gt_ctx_set_option(gt_ctx* ctx, const char* key, int value);
+
 /* Statistics of the last call on this context: fixed-point iterations of the
  * memory linker, fallback walks, candidates and particles. */
 typedef struct gt_stats {
@@ -143,6 +149,7 @@ typedef struct gt_stats {
     float ms_link;             /* linking incl. fixed-point passes and ids */
     float ms_assemble;         /* output table */
     float ms_total;            /* first to last kernel of the call */
+    int32_t locate_kernel;     /* 1 = specialised (TMA, f32x2) kernel, 0 = generic */
 } gt_stats;
 
 GT_API int gt_last_stats(const gt_ctx* ctx, gt_stats* out);

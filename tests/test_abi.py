@@ -27,7 +27,7 @@ def lib():
 def test_header_declares_entry_points():
     names = declared()
     for n in ["gt_batch", "gt_batch_device", "gt_link", "gt_ctx_create", "gt_ctx_destroy", "gt_last_error",
-              "gt_table_free", "gt_column_names", "gt_version", "gt_last_stats"]:
+              "gt_table_free", "gt_column_names", "gt_version", "gt_last_stats", "gt_ctx_set_option"]:
         assert n in names
 
 

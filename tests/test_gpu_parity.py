@@ -64,6 +64,7 @@ def test_plain_small_exact(gpu):
     mv = synth.make_movie(spec)
     params = dict(spec.params, cpu_processed=True)
     tab, cols = check(mv, **params)
+    assert _native.last_stats()["locate_kernel"] == 1, "specialised locate kernel not used"
     assert [c[0] for c in cols] == ["frame", "mass", "y", "x", "particle", "Rg", "ecc", "signal"]
     assert tab.shape[0] > 300
     pos_err, mass_err = fp64_error(tab, mv, dict(spec.params))
@@ -75,6 +76,7 @@ def test_plain_512_scaled_exact(gpu):
     spec = synth.scaled(synth.PLAIN_1000, frames=12)
     mv = synth.make_movie(spec)
     tab, _ = check(mv, **dict(spec.params, cpu_processed=True))
+    assert _native.last_stats()["locate_kernel"] == 1, "specialised locate kernel not used"
     assert tab.shape[0] > 12 * 300
 
 
@@ -169,6 +171,23 @@ def test_link_rust_matches_oracle(gpu):
     quirky = rows.copy()
     quirky[:, 0] += 3
     np.testing.assert_array_equal(link_rust(quirky, 6.0, 2), oracle.link(quirky, 6.0, 2))
+
+
+@pytest.mark.parametrize("opt", [("locate_tile_rows", 64), ("force_generic", 1)])
+def test_locate_kernel_variants_agree(gpu, opt):
+    """The specialised kernel at both tile heights and the generic kernel
+    produce identical tables."""
+    spec = synth.scaled(synth.PLAIN_1000, frames=6, seed=41)
+    mv = synth.make_movie(spec)
+    params = dict(spec.params, cpu_processed=True, characterize=True)
+    base = batch_rust(mv, **params)
+    try:
+        _native.set_option(*opt)
+        other = batch_rust(mv, **params)
+    finally:
+        _native.set_option("locate_tile_rows", 32)
+        _native.set_option("force_generic", 0)
+    assert_tables_equal(other, base, None)
 
 
 def test_full_size_plain_1000(gpu):

@@ -73,6 +73,7 @@ class GtStats(ctypes.Structure):
         ("ms_link", ctypes.c_float),
         ("ms_assemble", ctypes.c_float),
         ("ms_total", ctypes.c_float),
+        ("locate_kernel", ctypes.c_int32),
     ]
 
 
@@ -92,6 +93,7 @@ SIGNATURES = [
                                ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p]),
     ("gt_table_free", None, [ctypes.POINTER(GtTable)]),
     ("gt_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GtStats)]),
+    ("gt_ctx_set_option", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]),
 ]
 
 _lib = None
@@ -146,6 +148,12 @@ def check(status, ctx):
     if status == GT_ERR_ARG:
         raise ValueError(msg)
     raise GtError(status, msg)
+
+
+def set_option(key, value, device=0):
+    """Tuning knob of the device's context (gt_ctx_set_option)."""
+    ctx = context(device)
+    check(load().gt_ctx_set_option(ctx, key.encode(), int(value)), ctx)
 
 
 def last_stats(device=0):

@@ -33,7 +33,7 @@ __global__ void assemble_kernel(AsmArgs a);
 __global__ void grid_kernel(const float* py, const float* px, const int* npart, int cap_p, int G,
                             int ncy, int ncx, int* gstart, int* gidx);
 bool fast_supported(int kr, int dd);
-cudaError_t launch_locate_fast(int kr, int dd, dim3 grid, cudaStream_t st, const LocParams& p,
+cudaError_t launch_locate_fast(int kr, int dd, int th, dim3 grid, cudaStream_t st, const LocParams& p,
                                const MovieBufs& b, const FastGeo& g, const CUtensorMap& map, int frame0);
 cudaError_t launch_verify_division(float divisor, FixedDiv f, unsigned int* d_count, int num_sms,
                                    cudaStream_t st);
@@ -52,7 +52,8 @@ struct gt_ctx {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     std::map<uint32_t, bool> div_ok;  // divisor bits -> fast division verified exact
     unsigned int* d_count = nullptr;
-    int force_generic = 0;            // testing hook: always use locate_tiles_kernel
+    int force_generic = 0;            // always use locate_tiles_kernel
+    int fast_tile_rows = 32;          // output tile height of the fast kernel (32 or 64)
 };
 
 namespace {
@@ -205,7 +206,7 @@ void annulus_inds_f(float outer, float inner, std::vector<int>& off) {
 }
 
 int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int num_sms, Plan* pl,
-              std::string* msg, int force_generic_flag = 0) {
+              std::string* msg, int force_generic_flag = 0, int fast_tile_rows = 32) {
     Plan& P = *pl;
     P.T = T; P.H = H; P.W = W; P.dtype = dtype; P.r = r;
     LocParams& lp = P.lp;
@@ -236,17 +237,33 @@ int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int 
     lp.minmass = r.minmass;
     lp.hp = std::max({lp.o, lp.D - 1 - lp.o, lp.char_r, lp.rint_c + 2, 1});
     lp.TH = LOC_TH; lp.TW = LOC_TW;
+    lp.ntx = (W + lp.TW - 1) / lp.TW;
+    lp.nty = (H + lp.TH - 1) / lp.TH;
+    lp.dtype = dtype;
+    lp.cpu_processed = r.cpu_processed;
+    lp.characterize = r.characterize;
+    lp.zero_skip = lp.max_iter >= 1 && lp.rint_c <= lp.o && lp.rint_c <= lp.D - 1 - lp.o;
     P.fast = 0;
-    if (dtype == GT_U16 && fast_supported(lp.krad, lp.D) && lp.krad <= 7 && !force_generic_flag) {
+    float wmin = 1.0f;
+    for (int i = 0; i < lp.taps; ++i) wmin = std::min(wmin, lp.w[i]);
+    const bool want_fast = dtype == GT_U16 && fast_supported(lp.krad, lp.D) && lp.krad <= 7 &&
+                           !force_generic_flag && wmin >= std::ldexp(1.0f, -40);
+    P.char_tab.clear(); P.char_off.clear(); P.gchar_tab.clear();
+    circle_tables(lp.char_r, P.char_tab, &P.char_off, 1);
+    circle_tables(lp.rint_c, P.gchar_tab, nullptr, 0);
+    lp.n_char = (int)P.char_off.size() / 2;
+    lp.n_gchar = (int)P.gchar_tab.size() / 2;
+    if (want_fast) {
         FastGeo& g = P.fg;
         std::memset(&g, 0, sizeof(g));
         const int KR = lp.krad;
+        g.th = fast_tile_rows;
         g.hp = lp.hp + ((lp.hp - lp.o) & 1);  // keep hp - offset even (row pairs)
         g.L = (g.hp + KR + 7) / 8 * 8;
         g.hx = g.L - KR;
         g.RW = (g.L + 64 + g.hp + KR + 7) / 8 * 8;
-        g.RH = 64 + 2 * g.hp + 2 * KR;
-        g.PH = 64 + 2 * g.hp;
+        g.RH = g.th + 2 * g.hp + 2 * KR;
+        g.PH = g.th + 2 * g.hp;
         g.PW = g.RW - 2 * KR;
         g.NPW = (g.PW + 7) / 8;
         g.PWC = 8 * g.NPW;
@@ -256,42 +273,48 @@ int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int 
         g.GPS = odd(g.PWC);
         g.P2S = odd(g.PWC);
         g.RMS = odd(64);
+        int k1 = 0;
+        for (int i = -lp.rint_c; i <= lp.rint_c; ++i)
+            for (int j = -lp.rint_c; j <= lp.rint_c; ++j) k1 += (i * i + j * j <= lp.rint_c * lp.rint_c);
+        g.K1 = k1;
+        g.K2 = lp.n_char;
+        auto mag = [](int d) { return (unsigned int)((((unsigned long long)1 << 32) + d - 1) / d); };
+        g.mRW = mag(g.RW);
+        g.mRP = mag(g.RH / 2);
+        g.mPWC = mag(g.PWC);
+        g.mPP = mag(g.PH / 2);
         auto al = [](size_t x) { return (x + 127) / 128 * 128; };
-        const size_t u = al((size_t)g.RH * g.RW * 2);
         const size_t rp = al(std::max((size_t)(g.RH / 2) * g.RPS * 8, (size_t)(4 * g.NRQ) * g.P2S * 8));
-        const size_t gpb = al(std::max({(size_t)(4 * g.NRQ + KR) * g.GPS * 8, (size_t)(g.PH / 2 + 1) * g.RMS * 8,
-                                        (size_t)64 * 64 * 4, (size_t)64 * 64 + 4 * 4 * 512}));
-        g.off_rp = (int)u;
-        g.off_gp = (int)(u + rp);
-        g.off_bp = (int)(u + rp + gpb);
-        g.smem = (int)(u + rp + 2 * gpb);
-        if (g.smem <= 227 * 1024 && g.RW <= 256 && g.RH <= 256) {
+        const size_t gp = al(std::max({(size_t)(4 * g.NRQ + KR) * g.GPS * 8, (size_t)(g.PH / 2 + 1) * g.RMS * 8,
+                                       (size_t)g.th * 64 * 4}));
+        const size_t bp = al(std::max({(size_t)(4 * g.NRQ + KR) * g.GPS * 8, (size_t)g.RH * g.RW * 2,
+                                       (size_t)g.th * 64 + 4 * 4 * 512}));
+        const size_t t1 = al((size_t)g.K1 * 2 * 4 + (size_t)g.K1 * 8 + (size_t)g.K2 * 2 * 4);
+        const size_t t2 = al((size_t)g.K2 * 16);
+        g.off_rp = 0;
+        g.off_gp = (int)rp;
+        g.off_bp = (int)(rp + gp);
+        g.off_tab = (int)(rp + gp + bp);
+        g.off_tab2 = (int)(rp + gp + bp + t1);
+        g.smem = (int)(rp + gp + bp + t1 + t2);
+        if (g.smem <= 227 * 1024 && g.RW <= 256 && g.RH <= 256 && g.PWC * g.NRQ < 65536) {
             P.fast = 1;
-            lp.TH = 64;
+            lp.TH = g.th;
             lp.TW = 64;
+            lp.ntx = (W + lp.TW - 1) / lp.TW;
+            lp.nty = (H + lp.TH - 1) / lp.TH;
         }
     }
-    lp.ntx = (W + lp.TW - 1) / lp.TW;
-    lp.nty = (H + lp.TH - 1) / lp.TH;
-    lp.dtype = dtype;
-    lp.cpu_processed = r.cpu_processed;
-    lp.characterize = r.characterize;
-    lp.zero_skip = lp.max_iter >= 1 && lp.rint_c <= lp.o && lp.rint_c <= lp.D - 1 - lp.o;
-    P.char_tab.clear(); P.char_off.clear(); P.gchar_tab.clear();
-    circle_tables(lp.char_r, P.char_tab, &P.char_off, 1);
-    circle_tables(lp.rint_c, P.gchar_tab, nullptr, 0);
-    lp.n_char = (int)P.char_off.size() / 2;
-    lp.n_gchar = (int)P.gchar_tab.size() / 2;
     P.sig_off.clear(); P.bg_off.clear();
     if (r.has_sig) circle_inds_f(r.sig_radius, P.sig_off);
     if (r.has_bg) annulus_inds_f(r.bg_radius, r.sig_radius + r.gap_radius, P.bg_off);
     P.sep = (float)r.separation;
     P.link = r.has_search_range;
 
-    const int PH = lp.TH + 2 * lp.hp, PW = lp.TW + 2 * lp.hp;
+    const int PH = LOC_TH + 2 * lp.hp, PW = LOC_TW + 2 * lp.hp;  // generic kernel plan
     const int RH = PH + 2 * lp.krad, RW = PW + 2 * lp.krad;
     P.smem_loc = sizeof(float) * ((size_t)RH * RW + 2 * (size_t)RH * PW + (size_t)PH * PW) +
-                 sizeof(int) * (size_t)lp.TH * lp.TW + 4 * sizeof(float) * LOC_CMAX + (size_t)lp.TH * lp.TW;
+                 sizeof(int) * (size_t)LOC_TH * LOC_TW + 4 * sizeof(float) * LOC_CMAX + (size_t)LOC_TH * LOC_TW;
     P.smem_loc = (P.smem_loc + 15) / 16 * 16;
     if (P.smem_loc > 227 * 1024) { *msg = "diameter/separation too large for the tile plan"; return GT_ERR_ARG; }
     P.fb_win = std::min(FB_WIN_MAX, std::max(lp.rint_c + 1, lp.max_iter - 1 + lp.rint_c + 1));
@@ -609,24 +632,34 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
     for (int i = 0; i < 5; ++i)
         if (!ctx->ev[i]) CK(cudaEventCreate(&ctx->ev[i]));
     const int ntiles = P.lp.ntx * P.lp.nty;
-    if (P.fast) {
-        FastGeo g = P.fg;
+    bool fast = P.fast != 0;
+    FastGeo g = P.fg;
+    if (fast) {
         rc = fast_division(ctx, P, &g, st);
         if (rc) return rc;
+        fast = g.fastdiv != 0;  // otherwise the generic kernel (IEEE division)
+    }
+    ctx->stats.locate_kernel = fast ? 1 : 0;
+    if (fast) {
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
         g.use_tma = make_tensor_map(&map, d_frames, P) ? 1 : 0;
         CK(cudaEventRecord(ctx->ev[0], st));
         for (int f0 = 0; f0 < T; f0 += 65535) {
             dim3 grid(ntiles, std::min(65535, T - f0));
-            CK(launch_locate_fast(P.lp.krad, P.lp.D, grid, st, P.lp, b, g, map, f0));
+            CK(launch_locate_fast(P.lp.krad, P.lp.D, g.th, grid, st, P.lp, b, g, map, f0));
             ctx->stats.launches += 1;
         }
     } else {
+        LocParams lg = P.lp;  // generic tile plan (its own tile height)
+        lg.TH = LOC_TH;
+        lg.TW = LOC_TW;
+        lg.ntx = (P.W + LOC_TW - 1) / LOC_TW;
+        lg.nty = (P.H + LOC_TH - 1) / LOC_TH;
         CK(cudaEventRecord(ctx->ev[0], st));
         for (int f0 = 0; f0 < T; f0 += 65535) {
-            dim3 grid(ntiles, std::min(65535, T - f0));
-            locate_tiles_kernel<<<grid, 256, P.smem_loc, st>>>(P.lp, b, f0);
+            dim3 grid(lg.ntx * lg.nty, std::min(65535, T - f0));
+            locate_tiles_kernel<<<grid, 256, P.smem_loc, st>>>(lg, b, f0);
             ctx->stats.launches += 1;
         }
     }
@@ -724,7 +757,8 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
     CK(cudaSetDevice(ctx->device));
     for (int scale = 1; scale <= 64; scale *= 4) {
         Plan P;
-        rc = make_plan(r, T, H, W, dtype, scale, ctx->num_sms, &P, &ctx->err, ctx->force_generic);
+        rc = make_plan(r, T, H, W, dtype, scale, ctx->num_sms, &P, &ctx->err, ctx->force_generic,
+                       ctx->fast_tile_rows);
         if (rc) return rc;
         const size_t fbytes = host ? (size_t)T * H * W * elem_size(dtype) : 0;
         Work w{};
@@ -844,6 +878,15 @@ int gt_batch_device(gt_ctx* ctx, const void* d_frames, int dtype, int T, int H, 
                     const gt_params* params, float* d_out, int64_t out_rows, int64_t* nrows, void* stream) {
     cudaStream_t st = stream ? (cudaStream_t)stream : (ctx ? ctx->stream : nullptr);
     return batch_common(ctx, d_frames, false, dtype, T, H, W, params, nullptr, d_out, out_rows, nrows, st);
+}
+
+int gt_ctx_set_option(gt_ctx* ctx, const char* key, int value) {
+    if (!ctx || !key) return GT_ERR_ARG;
+    const std::string k(key);
+    if (k == "locate_tile_rows" && (value == 32 || value == 64)) { ctx->fast_tile_rows = value; return GT_OK; }
+    if (k == "force_generic" && (value == 0 || value == 1)) { ctx->force_generic = value; return GT_OK; }
+    ctx->err = "unknown option or value: " + k;
+    return GT_ERR_ARG;
 }
 
 void gt_table_free(gt_table* table) {

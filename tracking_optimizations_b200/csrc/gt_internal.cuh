@@ -82,7 +82,11 @@ struct FastGeo {
     int NPW, PWC;    // 8-column chunks of the row pass, columns computed
     int NRQ;         // 8-row chunks of the column pass
     int RPS, GPS, P2S, RMS;  // odd row-pair strides (float2 units)
-    int off_rp, off_gp, off_bp;  // byte offsets of the regions
+    int off_rp, off_gp, off_bp;  // byte offsets of the regions (raw u16 staged in bp)
+    int off_tab, off_tab2;       // circle tables
+    int K1, K2;                  // centroid circle and d/2 circle sizes
+    unsigned int mRW, mRP, mPWC, mPP;  // ceil(2^32 / x) for index division
+    int th;                      // output tile height (32 or 64)
     int smem;
     int use_tma;
     int fastdiv;

@@ -27,7 +27,7 @@
 namespace gt {
 
 namespace {
-constexpr int FT = 64;    // output tile edge
+constexpr int FT = 64;    // output tile width
 constexpr int FNT = 256;  // threads
 constexpr int FM = 8;     // outputs per thread item
 constexpr int FCMAX = 512;
@@ -110,18 +110,51 @@ struct P2Acc {  // processed plane held as row pairs, frame coordinates
     }
 };
 
-struct URawAcc {
-    const unsigned short* U;
-    int ry0, rx0, RW;
-    __device__ float operator()(int u, int v) const { return (float)U[(u - ry0) * RW + (v - rx0)]; }
+struct GRawAcc {  // raw pixels straight from the frame (characterize only)
+    const unsigned short* F;
+    int W;
+    __device__ float operator()(int u, int v) const { return (float)__ldg(F + (size_t)u * W + v); }
 };
+
+// floor(n / d) for n, d < 2^16 by one multiply-high (m = ceil(2^32 / d))
+__device__ __forceinline__ int fdiv16(int n, unsigned int m) { return (int)__umulhi((unsigned int)n, m); }
+
+// Centroid at (u, v) from the shared-memory tables (same order and
+// arithmetic as centroid_at).
+__device__ __forceinline__ bool centroid_tab(const LocParams& p, const P2Acc& P, const int* toff,
+                                             const float2* tij, int K, int u, int v, float& c0, float& c1,
+                                             float& m) {
+    const int bd = p.border;
+    if (u - bd < 0 || u + bd >= p.H || v - bd < 0 || v + bd >= p.W) {
+        c0 = 0.f; c1 = 0.f; m = 0.f;
+        return true;
+    }
+    const int rint = p.rint_c;
+    if (!P.covers(u - rint, v - rint) || !P.covers(u + rint, v + rint)) return false;
+    const int r0 = u - P.py0, cc = v - P.px0;
+    const int base = (((r0 >> 1) * P.S + cc) << 1);
+    const int* T = toff + (r0 & 1) * K;
+    float a0 = 0.f, a1 = 0.f, mm = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < K; ++k) {
+        const float data = P.P[base + T[k]];
+        const float2 ij = tij[k];
+        a0 = fmaf(data, ij.x, a0);
+        a1 = fmaf(data, ij.y, a1);
+        mm = mm + data;
+    }
+    c0 = a0 / mm;
+    c1 = a1 / mm;
+    m = mm;
+    return true;
+}
 
 __host__ __device__ constexpr int fast_offset(int DD) { return (int)((float)DD / 2.0f - 0.5f); }
 
 }  // namespace
 
-template <int KR, int DD>
-__global__ void __launch_bounds__(FNT, 2)
+template <int KR, int DD, int TH0>
+__global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     locate_fast_kernel(const LocParams p, const MovieBufs b, const FastGeo g,
                        const __grid_constant__ CUtensorMap tmap, int frame0) {
     constexpr int TAPS = 2 * KR + 1;
@@ -130,33 +163,38 @@ __global__ void __launch_bounds__(FNT, 2)
     __shared__ __align__(8) uint64_t bar;
     __shared__ int warp_tot[FNT / 32];
     __shared__ int s_total, s_base, s_fail;
-    __shared__ int rowcount[FT];
-    __shared__ int rowstart[FT];
+    __shared__ int rowcount[TH0];
+    __shared__ int rowstart[TH0];
 
     const int tid = threadIdx.x;
     const int tile = blockIdx.x;
     const int t = frame0 + blockIdx.y;
     const int ti = tile / p.ntx, tj = tile - ti * p.ntx;
-    const int ty0 = ti * FT, tx0 = tj * FT;
+    const int ty0 = ti * TH0, tx0 = tj * FT;
     const int H = p.H, W = p.W;
     const int hp = g.hp, hx = g.hx;
     const int RH = g.RH, RW = g.RW, PH = g.PH, PW = g.PW;
     const int ry0 = ty0 - hp - KR, rx0 = tx0 - g.L;
     const int py0 = ty0 - hp, px0 = tx0 - hx;
-    const int TH = min(FT, H - ty0);
+    const int TH = min(TH0, H - ty0);
 
-    unsigned short* U = (unsigned short*)smem;
     float2* Rp = (float2*)(smem + g.off_rp);
     float2* P2 = Rp;  // P2 replaces Rp once the row pass is done
     float2* Gp = (float2*)(smem + g.off_gp);
     float2* Bp = (float2*)(smem + g.off_bp);
+    unsigned short* U = (unsigned short*)Bp;   // raw tile until converted
     float2* RM2 = Gp;                          // after the column pass
     int* clist = (int*)Gp;                     // after the local-max pass
     unsigned char* flags = (unsigned char*)Bp;  // after the column pass
-    float* wy = (float*)(smem + g.off_bp + FT * FT);
+    float* wy = (float*)(smem + g.off_bp + TH0 * FT);
     float* wx = wy + FCMAX;
     float* wm = wx + FCMAX;
     int* wst = (int*)(wm + FCMAX);
+    // circle tables (persist through the tile)
+    int* ctoff = (int*)(smem + g.off_tab);            // 2 x K1: centroid offsets (even/odd base row)
+    float2* ctij = (float2*)(ctoff + 2 * g.K1);       // K1: (i, j)
+    int* xtoff = (int*)(ctij + g.K1);                 // 2 x K2: d/2 circle offsets
+    float4* xtab = (float4*)(smem + g.off_tab2);      // K2: (r2, sin2, cos2, 0)
 
     // ---- 0. stage the raw tile ----
     if (g.use_tma) {
@@ -180,7 +218,7 @@ __global__ void __launch_bounds__(FNT, 2)
     } else {
         const unsigned short* fr = (const unsigned short*)b.frames + (size_t)t * H * W;
         for (int i = tid; i < RH * RW; i += FNT) {
-            const int r = i / RW, c = i - r * RW;
+            const int r = fdiv16(i, g.mRW), c = i - r * RW;
             const int gy = ry0 + r, gx = rx0 + c;
             unsigned short v = 0;
             if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(fr + (size_t)gy * W + gx);
@@ -188,15 +226,37 @@ __global__ void __launch_bounds__(FNT, 2)
         }
         __syncthreads();
     }
-    if (tid < FT) {
+    if (tid < TH0) {
         rowstart[tid] = 0x7fffffff;
         rowcount[tid] = 0;
+    }
+    // offsets of the centroid circle (radius (d-1)/2, centers.wgsl order) and
+    // of the cpu_processed circle (radius d/2, kernels.rs order) in the row-pair
+    // layout, for an even (first half) and an odd (second half) base row
+    if (tid == 0) {
+        int k = 0;
+        const int rc = p.rint_c;
+        for (int i = -rc; i <= rc; ++i)
+            for (int j = -rc; j <= rc; ++j) {
+                const float x = (float)i, y = (float)j;
+                if (x * x + y * y > (float)rc * (float)rc) continue;
+                for (int e = 0; e < 2; ++e)
+                    ctoff[e * g.K1 + k] = ((((e + i) >> 1) * g.P2S + j) << 1) + ((e + i) & 1);
+                ctij[k] = make_float2(x, y);
+                ++k;
+            }
+    }
+    for (int k = tid; k < g.K2; k += FNT) {
+        const int i = __ldg(b.char_off + 2 * k), j = __ldg(b.char_off + 2 * k + 1);
+        for (int e = 0; e < 2; ++e) xtoff[e * g.K2 + k] = ((((e + i) >> 1) * g.P2S + j) << 1) + ((e + i) & 1);
+        xtab[k] = make_float4(__ldg(b.char_tab + 3 * k), __ldg(b.char_tab + 3 * k + 1),
+                              __ldg(b.char_tab + 3 * k + 2), 0.f);
     }
 
     // ---- 1. u16 -> f32 row pairs ----
     const int RP = RH >> 1;
     for (int i = tid; i < RP * RW; i += FNT) {
-        const int pr = i / RW, c = i - pr * RW;
+        const int pr = fdiv16(i, g.mRW), c = i - pr * RW;
         Rp[pr * g.RPS + c] = make_float2((float)U[(2 * pr) * RW + c], (float)U[(2 * pr + 1) * RW + c]);
     }
     __syncthreads();
@@ -204,11 +264,11 @@ __global__ void __launch_bounds__(FNT, 2)
     float2 W2[TAPS];
 #pragma unroll
     for (int j = 0; j < TAPS; ++j) W2[j] = make_float2(p.w[j], p.w[j]);
-    const bool fd = g.fastdiv != 0;
+    constexpr bool fd = true;  // the host verified the fixed-divisor division
 
     // ---- 2. row pass (preprocess_rows.wgsl) on row pairs ----
     for (int it = tid; it < RP * g.NPW; it += FNT) {
-        const int pr = it % RP, q = it / RP;
+        const int q = fdiv16(it, g.mRP), pr = it - q * RP;
         const int pc0 = q * FM;
         const float2* src = Rp + pr * g.RPS + pc0;
         float2 v[FM + 2 * KR];
@@ -254,7 +314,7 @@ __global__ void __launch_bounds__(FNT, 2)
     // ---- 3. column pass (preprocess_cols.wgsl) -> P2 ----
     const float NEG = -CUDART_INF_F;
     for (int it = tid; it < g.PWC * g.NRQ; it += FNT) {
-        const int c = it % g.PWC, rq = it / g.PWC;
+        const int rq = fdiv16(it, g.mPWC), c = it - rq * g.PWC;
         const int p0 = rq * (FM / 2);
         float2 L[FM / 2 + KR], ML[FM / 2 + KR - 1];
 #pragma unroll
@@ -318,7 +378,7 @@ __global__ void __launch_bounds__(FNT, 2)
     // ---- 4. row max over the dilation window (max_rows.wgsl) ----
     const int PP = PH >> 1;
     for (int it = tid; it < PP * (FT / FM); it += FNT) {
-        const int pr = it % PP, q = it / PP;
+        const int q = fdiv16(it, g.mPP), pr = it - q * PP;
         const int tc0 = q * FM;
         const float2* src = P2 + pr * g.P2S + tc0 + hx - O;
         float vx[FM + DD - 1], vy[FM + DD - 1];
@@ -337,7 +397,7 @@ __global__ void __launch_bounds__(FNT, 2)
     __syncthreads();
 
     // ---- 5. column max vs centre: non-strict local max (walk_cols.wgsl:19-36) ----
-    for (int it = tid; it < FT * (FT / FM); it += FNT) {
+    for (int it = tid; it < FT * (TH0 / FM); it += FNT) {
         const int tc = it % FT, rq = it / FT;
         const int tr0 = rq * FM;
         const int k0 = (tr0 + hp - O) >> 1;  // hp - O is even
@@ -367,16 +427,11 @@ __global__ void __launch_bounds__(FNT, 2)
     __syncthreads();
 
     // ---- 6. raster-order compaction, walks, emission ----
-    const int npx = FT * FT;
-    const int chunk = npx / FNT;
+    const int npx = TH0 * FT;
+    const int chunk = npx / FNT;  // 8 or 16 flags per thread
     const int q0 = tid * chunk;
     int mine = 0;
-    {
-        const uint4 fl = *(const uint4*)(flags + q0);  // chunk == 16 bytes
-        const unsigned char* fb = (const unsigned char*)&fl;
-#pragma unroll
-        for (int i = 0; i < 16; ++i) mine += fb[i];
-    }
+    for (int i = 0; i < chunk; ++i) mine += flags[q0 + i];
     int pos = block_excl_scan<FNT>(mine, warp_tot, &s_total);
     const int ncand = s_total;
     for (int q = q0; q < q0 + chunk; ++q)
@@ -384,11 +439,14 @@ __global__ void __launch_bounds__(FNT, 2)
     __syncthreads();
 
     P2Acc acc{(const float*)P2, py0, px0, PH, PW, g.P2S};
-    URawAcc racc{U, ry0, rx0, RW};
+    const unsigned short* frame = (const unsigned short*)b.frames + (size_t)t * H * W;
+    GRawAcc racc{frame, W};
+    // thread k serves candidate (k % 32) * 8 + k / 32: one lane per warp first
+    const int cidx = (tid & 31) * (FNT / 32) + (tid >> 5);
     int emitted = 0;
     for (int r0 = 0; r0 < ncand; r0 += FCMAX) {
         const int nr = min(FCMAX, ncand - r0);
-        for (int c = tid; c < nr; c += FNT) {
+        for (int c = cidx; c < nr; c += FNT) {
             const int q = clist[r0 + c];
             const int u0 = ty0 + q / FT, v0 = tx0 + q % FT;
             int st;
@@ -396,11 +454,25 @@ __global__ void __launch_bounds__(FNT, 2)
             if (p.max_iter <= 0) {
                 st = CAND_PENDING;
             } else {
-                WalkOut wo = walk_from(p, acc, u0, v0);
-                if (!wo.ok) {
+                // walk_cols.wgsl:38-74
+                int u = u0, v = v0;
+                float c0 = 0.f, c1 = 0.f;
+                bool ok = true;
+                for (int iter = 0; iter < p.max_iter; ++iter) {
+                    if (!centroid_tab(p, acc, ctoff, ctij, g.K1, u, v, c0, c1, m)) { ok = false; break; }
+                    bool changed = false;
+                    if (c0 > p.thr && u < H - 1) { u += 1; changed = true; }
+                    else if (c0 < -p.thr && u > 0) { u -= 1; changed = true; }
+                    if (c1 > p.thr && v < W - 1) { v += 1; changed = true; }
+                    else if (c1 < -p.thr && v > 0) { v -= 1; changed = true; }
+                    if (!changed) break;
+                }
+                if (!ok) {
                     st = CAND_PENDING;
+                    m = 0.f;
                 } else {
-                    y = wo.y; x = wo.x; m = wo.mass;
+                    y = (float)u + c0;
+                    x = (float)v + c1;
                     st = (m > p.minmass && m != 0.f) ? CAND_EMIT : CAND_REJECT;
                 }
             }
@@ -444,7 +516,46 @@ __global__ void __launch_bounds__(FNT, 2)
             rec.rg_sum = rec.eccn = rec.mid = rec.signal = 0.f;
             rec.g_rg = rec.g_raw = rec.g_sig = rec.g_ecc = 0.f;
             rec.pad = 0.f;
-            if (p.cpu_processed) cpu_features(p, b, acc, u0, v0, rec);
+            if (p.cpu_processed) {
+                // execute_gpu.rs:286-299: products summed per ndarray's
+                // eight-accumulator fold, all three sums in one pass
+                const int rr = u0 - py0, cc = v0 - px0;
+                const int base2 = (((rr >> 1) * g.P2S + cc) << 1);
+                const int* T = xtoff + (rr & 1) * g.K2;
+                const float* Pf = (const float*)P2;
+                float ar[8], as[8], ac[8];
+#pragma unroll
+                for (int l = 0; l < 8; ++l) { ar[l] = 0.f; as[l] = 0.f; ac[l] = 0.f; }
+                const int K = g.K2, K8 = K & ~7;
+                float sig = Pf[base2 + T[0]];
+                for (int k0 = 0; k0 < K8; k0 += 8) {
+#pragma unroll
+                    for (int l = 0; l < 8; ++l) {
+                        const float nb = Pf[base2 + T[k0 + l]];
+                        const float4 tb = xtab[k0 + l];
+                        ar[l] = ar[l] + nb * tb.x;
+                        as[l] = as[l] + nb * tb.y;
+                        ac[l] = ac[l] + nb * tb.z;
+                        sig = fmaxf(sig, nb);
+                    }
+                }
+                float rg = 0.f, sn = 0.f, cs = 0.f;
+                rg = rg + (ar[0] + ar[4]); rg = rg + (ar[1] + ar[5]); rg = rg + (ar[2] + ar[6]); rg = rg + (ar[3] + ar[7]);
+                sn = sn + (as[0] + as[4]); sn = sn + (as[1] + as[5]); sn = sn + (as[2] + as[6]); sn = sn + (as[3] + as[7]);
+                cs = cs + (ac[0] + ac[4]); cs = cs + (ac[1] + ac[5]); cs = cs + (ac[2] + ac[6]); cs = cs + (ac[3] + ac[7]);
+                for (int k = K8; k < K; ++k) {
+                    const float nb = Pf[base2 + T[k]];
+                    const float4 tb = xtab[k];
+                    rg = rg + nb * tb.x;
+                    sn = sn + nb * tb.y;
+                    cs = cs + nb * tb.z;
+                    sig = fmaxf(sig, nb);
+                }
+                rec.rg_sum = rg;
+                rec.eccn = sqrtf(sn * sn + cs * cs);
+                rec.mid = acc(u0, v0);
+                rec.signal = sig;
+            }
             if (p.characterize) gpu_features(p, b, acc, racc, u0, v0, rec);
             if (base >= 0) {
                 const int slot = base + epos;
@@ -462,12 +573,17 @@ __global__ void __launch_bounds__(FNT, 2)
     for (int r = tid; r < TH; r += FNT) b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = rowcount[r];
 }
 
-// Checks div1() against IEEE division for every positive finite binary32
-// dividend: the fast path is used for a divisor only if nothing differs.
+// Checks div1() against IEEE division for 0 and every binary32 dividend in
+// [2^-100, FLT_MAX].  Dividends of the fast kernel lie there: boxcar sums are
+// integers, and with every Gaussian weight >= 2^-40 (checked on the host) a
+// nonzero weighted sum of integer pixels is >= 2^-86.
 __global__ void verify_division_kernel(float divisor, FixedDiv f, unsigned int* mismatches) {
     const unsigned int stride = gridDim.x * blockDim.x;
     unsigned int bad = 0;
-    for (unsigned int bits = blockIdx.x * blockDim.x + threadIdx.x; bits < 0x7f800000u; bits += stride) {
+    const unsigned int lo = 0x0d800000u;  // 2^-100
+    const unsigned int tid0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid0 == 0) bad += (__float_as_uint(div1(0.f, f)) != __float_as_uint(__fdiv_rn(0.f, divisor)));
+    for (unsigned int bits = lo + tid0; bits < 0x7f800000u; bits += stride) {
         const float a = __uint_as_float(bits);
         const float want = __fdiv_rn(a, divisor);
         const float got = div1(a, f);
@@ -488,14 +604,21 @@ bool fast_supported(int kr, int dd) {
     return false;
 }
 
-cudaError_t launch_locate_fast(int kr, int dd, dim3 grid, cudaStream_t st, const LocParams& p,
+cudaError_t launch_locate_fast(int kr, int dd, int th, dim3 grid, cudaStream_t st, const LocParams& p,
                                const MovieBufs& b, const FastGeo& g, const CUtensorMap& map, int frame0) {
 #define GT_FAST_CASE(KR, DD)                                                                          \
     if (kr == KR && dd == DD) {                                                                       \
-        cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD>,                               \
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, g.smem);     \
-        if (e != cudaSuccess) return e;                                                               \
-        locate_fast_kernel<KR, DD><<<grid, FNT, g.smem, st>>>(p, b, g, map, frame0);                   \
+        if (th == 32) {                                                                               \
+            cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD, 32>,                       \
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, g.smem); \
+            if (e != cudaSuccess) return e;                                                           \
+            locate_fast_kernel<KR, DD, 32><<<grid, FNT, g.smem, st>>>(p, b, g, map, frame0);           \
+        } else {                                                                                      \
+            cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD, 64>,                       \
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, g.smem); \
+            if (e != cudaSuccess) return e;                                                           \
+            locate_fast_kernel<KR, DD, 64><<<grid, FNT, g.smem, st>>>(p, b, g, map, frame0);           \
+        }                                                                                             \
         return cudaGetLastError();                                                                    \
     }
     GT_FAST_LIST(GT_FAST_CASE)
