@@ -149,7 +149,7 @@ typedef struct gt_stats {
     float ms_link;             /* linking incl. fixed-point passes and ids */
     float ms_assemble;         /* output table */
     float ms_total;            /* first to last kernel of the call */
-    int32_t locate_kernel;     /* 1 = specialised (TMA, f32x2) kernel, 0 = generic */
+    int32_t locate_kernel;     /* 0 generic, 1 specialised, 2 specialised with TMA staging */
 } gt_stats;
 
 GT_API int gt_last_stats(const gt_ctx* ctx, gt_stats* out);

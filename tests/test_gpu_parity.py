@@ -64,7 +64,7 @@ def test_plain_small_exact(gpu):
     mv = synth.make_movie(spec)
     params = dict(spec.params, cpu_processed=True)
     tab, cols = check(mv, **params)
-    assert _native.last_stats()["locate_kernel"] == 1, "specialised locate kernel not used"
+    assert _native.last_stats()["locate_kernel"] == 2, "specialised TMA locate kernel not used"
     assert [c[0] for c in cols] == ["frame", "mass", "y", "x", "particle", "Rg", "ecc", "signal"]
     assert tab.shape[0] > 300
     pos_err, mass_err = fp64_error(tab, mv, dict(spec.params))
@@ -76,7 +76,7 @@ def test_plain_512_scaled_exact(gpu):
     spec = synth.scaled(synth.PLAIN_1000, frames=12)
     mv = synth.make_movie(spec)
     tab, _ = check(mv, **dict(spec.params, cpu_processed=True))
-    assert _native.last_stats()["locate_kernel"] == 1, "specialised locate kernel not used"
+    assert _native.last_stats()["locate_kernel"] == 2, "specialised TMA locate kernel not used"
     assert tab.shape[0] > 12 * 300
 
 

@@ -32,9 +32,10 @@ __global__ void newid_kernel(const int* newrank, const int* newbase, const int* 
 __global__ void assemble_kernel(AsmArgs a);
 __global__ void grid_kernel(const float* py, const float* px, const int* npart, int cap_p, int G,
                             int ncy, int ncx, int* gstart, int* gidx);
-bool fast_supported(int kr, int dd);
-cudaError_t launch_locate_fast(int kr, int dd, int th, dim3 grid, cudaStream_t st, const LocParams& p,
-                               const MovieBufs& b, const FastGeo& g, const CUtensorMap& map, int frame0);
+bool fast_supported(int kr, int dd, int rc, int diameter);
+cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaStream_t st, const LocParams& p,
+                               const MovieBufs& b, FixedDiv dnorm, FixedDiv dkk, int T, int frame0,
+                               int* used_tma);
 cudaError_t launch_verify_division(float divisor, FixedDiv f, unsigned int* d_count, int num_sms,
                                    cudaStream_t st);
 }  // namespace gt
@@ -166,7 +167,7 @@ struct Plan {
     size_t smem_loc = 0, smem_fb = 0, smem_fin = 0;
     int fb_win = 0;
     int fast = 0;
-    FastGeo fg{};
+    int fast_th = 32;
     std::vector<float> char_tab, gchar_tab;
     std::vector<int> char_off, sig_off, bg_off;
     std::vector<std::string> names, types;
@@ -246,7 +247,7 @@ int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int 
     P.fast = 0;
     float wmin = 1.0f;
     for (int i = 0; i < lp.taps; ++i) wmin = std::min(wmin, lp.w[i]);
-    const bool want_fast = dtype == GT_U16 && fast_supported(lp.krad, lp.D) && lp.krad <= 7 &&
+    const bool want_fast = dtype == GT_U16 && fast_supported(lp.krad, lp.D, lp.rint_c, lp.d) &&
                            !force_generic_flag && wmin >= std::ldexp(1.0f, -40);
     P.char_tab.clear(); P.char_off.clear(); P.gchar_tab.clear();
     circle_tables(lp.char_r, P.char_tab, &P.char_off, 1);
@@ -254,56 +255,12 @@ int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int 
     lp.n_char = (int)P.char_off.size() / 2;
     lp.n_gchar = (int)P.gchar_tab.size() / 2;
     if (want_fast) {
-        FastGeo& g = P.fg;
-        std::memset(&g, 0, sizeof(g));
-        const int KR = lp.krad;
-        g.th = fast_tile_rows;
-        g.hp = lp.hp + ((lp.hp - lp.o) & 1);  // keep hp - offset even (row pairs)
-        g.L = (g.hp + KR + 7) / 8 * 8;
-        g.hx = g.L - KR;
-        g.RW = (g.L + 64 + g.hp + KR + 7) / 8 * 8;
-        g.RH = g.th + 2 * g.hp + 2 * KR;
-        g.PH = g.th + 2 * g.hp;
-        g.PW = g.RW - 2 * KR;
-        g.NPW = (g.PW + 7) / 8;
-        g.PWC = 8 * g.NPW;
-        g.NRQ = (g.PH + 7) / 8;
-        auto odd = [](int x) { return x | 1; };
-        g.RPS = odd(g.PWC + 2 * KR);
-        g.GPS = odd(g.PWC);
-        g.P2S = odd(g.PWC);
-        g.RMS = odd(64);
-        int k1 = 0;
-        for (int i = -lp.rint_c; i <= lp.rint_c; ++i)
-            for (int j = -lp.rint_c; j <= lp.rint_c; ++j) k1 += (i * i + j * j <= lp.rint_c * lp.rint_c);
-        g.K1 = k1;
-        g.K2 = lp.n_char;
-        auto mag = [](int d) { return (unsigned int)((((unsigned long long)1 << 32) + d - 1) / d); };
-        g.mRW = mag(g.RW);
-        g.mRP = mag(g.RH / 2);
-        g.mPWC = mag(g.PWC);
-        g.mPP = mag(g.PH / 2);
-        auto al = [](size_t x) { return (x + 127) / 128 * 128; };
-        const size_t rp = al(std::max((size_t)(g.RH / 2) * g.RPS * 8, (size_t)(4 * g.NRQ) * g.P2S * 8));
-        const size_t gp = al(std::max({(size_t)(4 * g.NRQ + KR) * g.GPS * 8, (size_t)(g.PH / 2 + 1) * g.RMS * 8,
-                                       (size_t)g.th * 64 * 4}));
-        const size_t bp = al(std::max({(size_t)(4 * g.NRQ + KR) * g.GPS * 8, (size_t)g.RH * g.RW * 2,
-                                       (size_t)g.th * 64 + 4 * 4 * 512}));
-        const size_t t1 = al((size_t)g.K1 * 2 * 4 + (size_t)g.K1 * 8 + (size_t)g.K2 * 2 * 4);
-        const size_t t2 = al((size_t)g.K2 * 16);
-        g.off_rp = 0;
-        g.off_gp = (int)rp;
-        g.off_bp = (int)(rp + gp);
-        g.off_tab = (int)(rp + gp + bp);
-        g.off_tab2 = (int)(rp + gp + bp + t1);
-        g.smem = (int)(rp + gp + bp + t1 + t2);
-        if (g.smem <= 227 * 1024 && g.RW <= 256 && g.RH <= 256 && g.PWC * g.NRQ < 65536) {
-            P.fast = 1;
-            lp.TH = g.th;
-            lp.TW = 64;
-            lp.ntx = (W + lp.TW - 1) / lp.TW;
-            lp.nty = (H + lp.TH - 1) / lp.TH;
-        }
+        P.fast = 1;
+        P.fast_th = fast_tile_rows;
+        lp.TH = fast_tile_rows;
+        lp.TW = 64;
+        lp.ntx = (W + lp.TW - 1) / lp.TW;
+        lp.nty = (H + lp.TH - 1) / lp.TH;
     }
     P.sig_off.clear(); P.bg_off.clear();
     if (r.has_sig) circle_inds_f(r.sig_radius, P.sig_off);
@@ -566,8 +523,8 @@ MovieBufs movie_bufs(const Plan& P, const Work& w, const void* frames) {
 }
 
 // Exhaustive check (cached per divisor) that the fixed-divisor division of
-// the fast kernel equals IEEE division for every positive binary32 dividend.
-int fast_division(gt_ctx* ctx, const Plan& P, FastGeo* g, cudaStream_t st) {
+// the fast kernel equals IEEE division on its dividend domain.
+int fast_division(gt_ctx* ctx, const Plan& P, FixedDiv* dn, FixedDiv* dk, bool* ok, cudaStream_t st) {
     const float divs[2] = {P.lp.norm, P.lp.kk};
     FixedDiv fdv[2];
     bool all = true;
@@ -589,33 +546,10 @@ int fast_division(gt_ctx* ctx, const Plan& P, FastGeo* g, cudaStream_t st) {
         }
         all = all && it->second;
     }
-    g->fastdiv = all ? 1 : 0;
-    g->dnorm = fdv[0];
-    g->dkk = fdv[1];
+    *ok = all;
+    *dn = fdv[0];
+    *dk = fdv[1];
     return GT_OK;
-}
-
-// TMA descriptor over the movie (u16, dims W x H x T).  Needs a 16-byte
-// aligned base and a row pitch that is a multiple of 16 bytes.
-bool make_tensor_map(CUtensorMap* map, const void* frames, const Plan& P) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
-        void* fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn)
-            return false;
-        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-    }
-    if (((uintptr_t)frames & 15) || (P.W * 2) % 16) return false;
-    cuuint64_t dims[3] = {(cuuint64_t)P.W, (cuuint64_t)P.H, (cuuint64_t)P.T};
-    cuuint64_t strides[2] = {(cuuint64_t)P.W * 2, (cuuint64_t)P.W * P.H * 2};
-    cuuint32_t box[3] = {(cuuint32_t)P.fg.RW, (cuuint32_t)P.fg.RH, 1};
-    cuuint32_t es[3] = {1, 1, 1};
-    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, const_cast<void*>(frames), dims, strides, box, es,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
 }
 
 // The whole locate(+link) pipeline on device frames; table left in w.out.
@@ -633,22 +567,23 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
         if (!ctx->ev[i]) CK(cudaEventCreate(&ctx->ev[i]));
     const int ntiles = P.lp.ntx * P.lp.nty;
     bool fast = P.fast != 0;
-    FastGeo g = P.fg;
+    FixedDiv dn{}, dk{};
     if (fast) {
-        rc = fast_division(ctx, P, &g, st);
+        bool ok = false;
+        rc = fast_division(ctx, P, &dn, &dk, &ok, st);
         if (rc) return rc;
-        fast = g.fastdiv != 0;  // otherwise the generic kernel (IEEE division)
+        fast = ok;  // otherwise the generic kernel (IEEE division)
     }
     ctx->stats.locate_kernel = fast ? 1 : 0;
     if (fast) {
-        CUtensorMap map;
-        std::memset(&map, 0, sizeof(map));
-        g.use_tma = make_tensor_map(&map, d_frames, P) ? 1 : 0;
         CK(cudaEventRecord(ctx->ev[0], st));
         for (int f0 = 0; f0 < T; f0 += 65535) {
             dim3 grid(ntiles, std::min(65535, T - f0));
-            CK(launch_locate_fast(P.lp.krad, P.lp.D, g.th, grid, st, P.lp, b, g, map, f0));
+            int used_tma = 0;
+            CK(launch_locate_fast(P.lp.krad, P.lp.D, P.lp.rint_c, P.fast_th, grid, st, P.lp, b, dn, dk, T, f0,
+                                  &used_tma));
             ctx->stats.launches += 1;
+            ctx->stats.locate_kernel = used_tma ? 2 : 1;
         }
     } else {
         LocParams lg = P.lp;  // generic tile plan (its own tile height)

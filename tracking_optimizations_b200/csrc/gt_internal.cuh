@@ -72,26 +72,7 @@ struct FixedDiv {
     float nb;
 };
 
-// Geometry of the fast locate kernel (64 x 64 output tiles).
-struct FastGeo {
-    int hp;          // processed halo above/below the tile (hp - offset even)
-    int L;           // raw columns left of the tile (multiple of 8)
-    int hx;          // processed columns left of the tile (L - krad)
-    int RH, RW;      // raw region (u16 staging, RW multiple of 8)
-    int PH, PW;      // processed region
-    int NPW, PWC;    // 8-column chunks of the row pass, columns computed
-    int NRQ;         // 8-row chunks of the column pass
-    int RPS, GPS, P2S, RMS;  // odd row-pair strides (float2 units)
-    int off_rp, off_gp, off_bp;  // byte offsets of the regions (raw u16 staged in bp)
-    int off_tab, off_tab2;       // circle tables
-    int K1, K2;                  // centroid circle and d/2 circle sizes
-    unsigned int mRW, mRP, mPWC, mPP;  // ceil(2^32 / x) for index division
-    int th;                      // output tile height (32 or 64)
-    int smem;
-    int use_tma;
-    int fastdiv;
-    FixedDiv dnorm, dkk;
-};
+
 
 // Per-movie device buffers and capacities.
 struct MovieBufs {

@@ -1,25 +1,32 @@
-// locate_fast.cu -- instruction-lean locate kernel for sm_100a.
+// locate_fast.cu -- specialised locate kernel for sm_100a.
 //
 // Same results, bit for bit, as locate_tiles_kernel (and the oracle): the
-// per-pixel arithmetic chains are unchanged, only packed two per f32x2
+// per-pixel arithmetic chains are unchanged, only packed two per FP32x2
 // instruction, and the boxcar of uint16 frames uses running sums, which are
 // exact because every partial sum is an integer below 2^24.
 //
-// One CTA per (frame, 64 x 64 output tile), 256 threads, 2 CTAs per SM:
+// Specialised on (smoothing radius KR, dilation size DD, tile height TH0,
+// centroid radius RC with diameter 2*RC + 1), so the whole tile geometry is
+// known at compile time: every shared-memory offset is an immediate and
+// every loop has a constant trip count.  One CTA per (frame, TH0 x 64 output
+// tile), 256 threads:
 //   0. the uint16 tile plus halo is staged by one TMA load (zero fill
 //      outside the frame) into U[RH][RW];
 //   1. U -> Rp: f32, rows interleaved in pairs (float2 = rows 2p, 2p+1);
-//   2. row pass: a thread filters one row pair over 8 columns (f32x2 FMA
-//      chains in tap order), Gaussian and boxcar -> Gp, Bp (row pairs);
+//   2. row pass: a thread filters one row pair over 8 columns (FFMA2 chains
+//      in tap order), Gaussian and boxcar -> Gp, Bp (row pairs);
 //   3. column pass: a thread filters one column over 8 rows (4 row pairs),
 //      divides by the Gaussian norm and k^2, clips at 0 -> P2 (row pairs);
 //   4. row max over the dilation window (register sliding max) -> RM2;
 //   5. column max of RM2 compared with the centre -> local-max flags;
-//   6. flagged pixels are compacted in raster order, walked and emitted as
-//      in locate_tiles_kernel.
+//   6. flagged pixels are compacted in raster order; the tile's candidates
+//      share one warp for the walk, the features and the emission.
 // Row strides of the pair arrays are odd (in 8-byte units), so every
 // lane-per-row access is bank-conflict free.
 #include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
 
 #include "gt_device.cuh"
 #include "gt_simd.cuh"
@@ -31,6 +38,63 @@ constexpr int FT = 64;    // output tile width
 constexpr int FNT = 256;  // threads
 constexpr int FM = 8;     // outputs per thread item
 constexpr int FCMAX = 512;
+
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int round8(int x) { return (x + 7) / 8 * 8; }
+__host__ __device__ constexpr int align128(int x) { return (x + 127) / 128 * 128; }
+__host__ __device__ constexpr int fast_offset(int DD) { return (int)((float)DD / 2.0f - 0.5f); }
+__host__ __device__ constexpr int circle_size(int RC) {
+    int k = 0;
+    for (int i = -RC; i <= RC; ++i)
+        for (int j = -RC; j <= RC; ++j) k += (i * i + j * j <= RC * RC);
+    return k;
+}
+
+// Compile-time tile geometry.
+template <int KR, int DD, int TH0, int RC>
+struct Geo {
+    static constexpr int O = fast_offset(DD);
+    static constexpr int HP0 = cmax(cmax(O, DD - 1 - O), cmax(RC + 2, 1));  // d/2 == RC for odd d
+    static constexpr int HP = HP0 + ((HP0 - O) & 1);  // hp - O even: row pairs align
+    static constexpr int L = round8(HP + KR);        // raw columns left of the tile
+    static constexpr int HX = L - KR;                // processed columns left of the tile
+    static constexpr int RW = round8(L + FT + HP + KR);
+    static constexpr int RH = TH0 + 2 * HP + 2 * KR;
+    static constexpr int RP = RH / 2;
+    static constexpr int PH = TH0 + 2 * HP;
+    static constexpr int PP = PH / 2;
+    static constexpr int PW = RW - 2 * KR;
+    static constexpr int NPW = (PW + FM - 1) / FM;
+    static constexpr int PWC = FM * NPW;
+    static constexpr int NRQ = (PH + FM - 1) / FM;
+    static constexpr int RPS = (PWC + 2 * KR) | 1;
+    static constexpr int GPS = PWC | 1;
+    static constexpr int P2S = PWC | 1;
+    static constexpr int RMS = FT | 1;
+    static constexpr int RPA = 4 * NRQ + KR;  // Gp/Bp row pairs allocated
+    static constexpr int SZ_RP = align128(cmax(RP * RPS * 8, 4 * NRQ * P2S * 8));
+    static constexpr int SZ_GP = align128(cmax(cmax(RPA * GPS * 8, (PP + 1) * RMS * 8), TH0 * FT * 4));
+    static constexpr int SZ_BP = align128(cmax(cmax(RPA * GPS * 8, RH * RW * 2), TH0 * FT + 4 * 4 * FCMAX));
+    static constexpr int K = circle_size(RC);
+    static constexpr int SZ_TAB = align128(K * 8);
+    static constexpr int OFF_GP = SZ_RP;
+    static constexpr int OFF_BP = SZ_RP + SZ_GP;
+    static constexpr int OFF_TAB = SZ_RP + SZ_GP + SZ_BP;
+    static constexpr int SMEM = OFF_TAB + SZ_TAB;
+    // index invariants of the phases below
+    static_assert(((HP - O) & 1) == 0, "row pairs of the local-max pass must align");
+    static_assert(HX >= HP && HX - O >= 0, "row max window starts inside the processed region");
+    static_assert(FT - 1 + HX + (DD - 1 - O) <= PW - 1, "row max window ends inside the computed columns");
+    static_assert(((TH0 - FM + HP - O) >> 1) + (FM + DD) / 2 - 1 <= PP, "column max rows allocated");
+    static_assert(TH0 - 1 + HP + (DD - 1 - O) <= PH - 1, "column max window inside the processed rows");
+    static_assert(FT + HX <= PW, "centre columns computed");
+    static_assert(4 * (NRQ - 1) + FM / 2 + KR <= RPA, "column pass reads allocated row pairs");
+    static_assert((PH - 2) / 2 + KR <= RP - 1, "valid outputs read computed row pairs only");
+    static_assert(PWC + 2 * KR <= RPS && PWC <= GPS && PWC <= P2S && FT <= RMS, "row strides");
+    static_assert(RW <= 256 && RH <= 256, "TMA box");
+    static_assert(SMEM <= 227 * 1024, "shared memory");
+    static_assert(RC + 2 <= HP && RC <= HX, "walk and feature circles inside the processed region");
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -69,10 +133,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // max over v[m .. m+DD-1] for m = 0..M-1, sharing the common core
 template <int DD, int M>
 __device__ __forceinline__ void slide_max(const float (&v)[M + DD - 1], float (&out)[M]) {
-    if constexpr (DD <= 0) {
-#pragma unroll
-        for (int m = 0; m < M; ++m) out[m] = -CUDART_INF_F;
-    } else if constexpr (DD < M) {
+    if constexpr (DD < M) {
 #pragma unroll
         for (int m = 0; m < M; ++m) {
             float x = v[m];
@@ -97,16 +158,18 @@ __device__ __forceinline__ void slide_max(const float (&v)[M + DD - 1], float (&
     }
 }
 
-struct P2Acc {  // processed plane held as row pairs, frame coordinates
-    const float* P;  // float view of the float2 array
-    int py0, px0, PH, PW, S;  // S = row-pair stride in float2
+// processed plane as row pairs, frame coordinates, compile-time geometry
+template <class G>
+struct P2Acc {
+    const float* P;
+    int py0, px0;
     __device__ bool covers(int u, int v) const {
         const int r = u - py0, c = v - px0;
-        return r >= 0 && r < PH && c >= 0 && c < PW;
+        return r >= 0 && r < G::PH && c >= 0 && c < G::PW;
     }
     __device__ float operator()(int u, int v) const {
         const int r = u - py0, c = v - px0;
-        return P[(((r >> 1) * S + c) << 1) + (r & 1)];
+        return P[(((r >> 1) * G::P2S + c) << 1) + (r & 1)];
     }
 };
 
@@ -116,49 +179,104 @@ struct GRawAcc {  // raw pixels straight from the frame (characterize only)
     __device__ float operator()(int u, int v) const { return (float)__ldg(F + (size_t)u * W + v); }
 };
 
-// floor(n / d) for n, d < 2^16 by one multiply-high (m = ceil(2^32 / d))
-__device__ __forceinline__ int fdiv16(int n, unsigned int m) { return (int)__umulhi((unsigned int)n, m); }
+// Centroid sums at a centre whose processed row has parity E, fully unrolled
+// (centers.wgsl:39-85 order: i outer, j inner, mask x^2 + y^2 <= r^2).
+template <int RC, int E, int S>
+__device__ __forceinline__ void circle_centroid(const float* P, int base, float& a0, float& a1, float& mm) {
+#pragma unroll
+    for (int i = -RC; i <= RC; ++i) {
+#pragma unroll
+        for (int j = -RC; j <= RC; ++j) {
+            if (i * i + j * j > RC * RC) continue;
+            const float data = P[base + ((((E + i) >> 1) * S + j) << 1) + ((E + i) & 1)];
+            a0 = fmaf(data, (float)i, a0);
+            a1 = fmaf(data, (float)j, a1);
+            mm = mm + data;
+        }
+    }
+}
 
-// Centroid at (u, v) from the shared-memory tables (same order and
-// arithmetic as centroid_at).
-__device__ __forceinline__ bool centroid_tab(const LocParams& p, const P2Acc& P, const int* toff,
-                                             const float2* tij, int K, int u, int v, float& c0, float& c1,
-                                             float& m) {
+// eight-lane fold of ndarray's unrolled_fold: acc = 0 + (p0+p4) + (p1+p5) + ...
+__device__ __forceinline__ float fold8(const float (&a)[8]) {
+    float acc = 0.f;
+    acc = acc + (a[0] + a[4]);
+    acc = acc + (a[1] + a[5]);
+    acc = acc + (a[2] + a[6]);
+    acc = acc + (a[3] + a[7]);
+    return acc;
+}
+
+// cpu_processed sums of processed * {r2, sin2, cos2} over the d/2 circle
+// (equal to the centroid circle for odd d), products folded as ndarray's
+// sum_axis does (execute_gpu.rs:289-291), fully unrolled.
+template <int RC, int E, int S>
+__device__ __forceinline__ void circle_features(const float* P, int base, const float2* sc, float& rg, float& sn,
+                                                float& cs, float& sig) {
+    constexpr int K = circle_size(RC);
+    constexpr int K8 = K & ~7;
+    float ar[8], as[8], ac[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) { ar[l] = 0.f; as[l] = 0.f; ac[l] = 0.f; }
+    float tr = 0.f, ts = 0.f, tc = 0.f;
+    sig = -CUDART_INF_F;
+    int q = 0;
+#pragma unroll
+    for (int i = -RC; i <= RC; ++i) {
+#pragma unroll
+        for (int j = -RC; j <= RC; ++j) {
+            if (i * i + j * j > RC * RC) continue;
+            const float nb = P[base + ((((E + i) >> 1) * S + j) << 1) + ((E + i) & 1)];
+            const float2 t = sc[q];
+            const float pr = nb * (float)(i * i + j * j), ps = nb * t.x, pc = nb * t.y;
+            sig = fmaxf(sig, nb);
+            if (q < K8) {
+                ar[q & 7] = ar[q & 7] + pr;
+                as[q & 7] = as[q & 7] + ps;
+                ac[q & 7] = ac[q & 7] + pc;
+                if (q == K8 - 1) { tr = fold8(ar); ts = fold8(as); tc = fold8(ac); }
+            } else {
+                tr = tr + pr;
+                ts = ts + ps;
+                tc = tc + pc;
+            }
+            ++q;
+        }
+    }
+    rg = tr;
+    sn = ts;
+    cs = tc;
+}
+
+template <class G, int RC>
+__device__ __forceinline__ bool centroid_fixed(const LocParams& p, const P2Acc<G>& P, int u, int v, float& c0,
+                                               float& c1, float& m) {
     const int bd = p.border;
     if (u - bd < 0 || u + bd >= p.H || v - bd < 0 || v + bd >= p.W) {
         c0 = 0.f; c1 = 0.f; m = 0.f;
         return true;
     }
-    const int rint = p.rint_c;
-    if (!P.covers(u - rint, v - rint) || !P.covers(u + rint, v + rint)) return false;
+    if (!P.covers(u - RC, v - RC) || !P.covers(u + RC, v + RC)) return false;
     const int r0 = u - P.py0, cc = v - P.px0;
-    const int base = (((r0 >> 1) * P.S + cc) << 1);
-    const int* T = toff + (r0 & 1) * K;
+    const int base = (((r0 >> 1) * G::P2S + cc) << 1);
     float a0 = 0.f, a1 = 0.f, mm = 0.f;
-#pragma unroll 4
-    for (int k = 0; k < K; ++k) {
-        const float data = P.P[base + T[k]];
-        const float2 ij = tij[k];
-        a0 = fmaf(data, ij.x, a0);
-        a1 = fmaf(data, ij.y, a1);
-        mm = mm + data;
-    }
+    if (r0 & 1) circle_centroid<RC, 1, G::P2S>(P.P, base, a0, a1, mm);
+    else circle_centroid<RC, 0, G::P2S>(P.P, base, a0, a1, mm);
     c0 = a0 / mm;
     c1 = a1 / mm;
     m = mm;
     return true;
 }
 
-__host__ __device__ constexpr int fast_offset(int DD) { return (int)((float)DD / 2.0f - 0.5f); }
-
 }  // namespace
 
-template <int KR, int DD, int TH0>
+template <int KR, int DD, int TH0, int RC>
 __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
-    locate_fast_kernel(const LocParams p, const MovieBufs b, const FastGeo g,
-                       const __grid_constant__ CUtensorMap tmap, int frame0) {
+    locate_fast_kernel(const LocParams p, const MovieBufs b, const FixedDiv dnorm, const FixedDiv dkk,
+                       const __grid_constant__ CUtensorMap tmap, int use_tma, int frame0) {
+    using G = Geo<KR, DD, TH0, RC>;
     constexpr int TAPS = 2 * KR + 1;
-    constexpr int O = fast_offset(DD);
+    constexpr int O = G::O;
+    constexpr int HP = G::HP, HX = G::HX;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ int warp_tot[FNT / 32];
@@ -172,39 +290,33 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     const int ti = tile / p.ntx, tj = tile - ti * p.ntx;
     const int ty0 = ti * TH0, tx0 = tj * FT;
     const int H = p.H, W = p.W;
-    const int hp = g.hp, hx = g.hx;
-    const int RH = g.RH, RW = g.RW, PH = g.PH, PW = g.PW;
-    const int ry0 = ty0 - hp - KR, rx0 = tx0 - g.L;
-    const int py0 = ty0 - hp, px0 = tx0 - hx;
+    const int ry0 = ty0 - HP - KR, rx0 = tx0 - G::L;
+    const int py0 = ty0 - HP, px0 = tx0 - HX;
     const int TH = min(TH0, H - ty0);
 
-    float2* Rp = (float2*)(smem + g.off_rp);
+    float2* Rp = (float2*)smem;
     float2* P2 = Rp;  // P2 replaces Rp once the row pass is done
-    float2* Gp = (float2*)(smem + g.off_gp);
-    float2* Bp = (float2*)(smem + g.off_bp);
-    unsigned short* U = (unsigned short*)Bp;   // raw tile until converted
-    float2* RM2 = Gp;                          // after the column pass
-    int* clist = (int*)Gp;                     // after the local-max pass
+    float2* Gp = (float2*)(smem + G::OFF_GP);
+    float2* Bp = (float2*)(smem + G::OFF_BP);
+    unsigned short* U = (unsigned short*)Bp;    // raw tile until converted
+    float2* RM2 = Gp;                           // after the column pass
+    int* clist = (int*)Gp;                      // after the local-max pass
     unsigned char* flags = (unsigned char*)Bp;  // after the column pass
-    float* wy = (float*)(smem + g.off_bp + TH0 * FT);
+    float* wy = (float*)(smem + G::OFF_BP + TH0 * FT);
     float* wx = wy + FCMAX;
     float* wm = wx + FCMAX;
     int* wst = (int*)(wm + FCMAX);
-    // circle tables (persist through the tile)
-    int* ctoff = (int*)(smem + g.off_tab);            // 2 x K1: centroid offsets (even/odd base row)
-    float2* ctij = (float2*)(ctoff + 2 * g.K1);       // K1: (i, j)
-    int* xtoff = (int*)(ctij + g.K1);                 // 2 x K2: d/2 circle offsets
-    float4* xtab = (float4*)(smem + g.off_tab2);      // K2: (r2, sin2, cos2, 0)
+    float2* sc = (float2*)(smem + G::OFF_TAB);  // (sin2, cos2) of the d/2 circle
 
     // ---- 0. stage the raw tile ----
-    if (g.use_tma) {
+    if (use_tma) {
         if (tid == 0) {
             mbar_init(&bar, 1);
             s_fail = 0;
         }
         __syncthreads();
         if (tid == 0) {
-            mbar_expect_tx(&bar, (uint32_t)(RH * RW * 2));
+            mbar_expect_tx(&bar, (uint32_t)(G::RH * G::RW * 2));
             tma_load_3d(U, &tmap, &bar, rx0, ry0, t);
             bool done = false;
             for (int it = 0; it < (1 << 22) && !done; ++it) done = mbar_try_wait(&bar, 0);
@@ -217,8 +329,8 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
         if (s_fail) return;
     } else {
         const unsigned short* fr = (const unsigned short*)b.frames + (size_t)t * H * W;
-        for (int i = tid; i < RH * RW; i += FNT) {
-            const int r = fdiv16(i, g.mRW), c = i - r * RW;
+        for (int i = tid; i < G::RH * G::RW; i += FNT) {
+            const int r = i / G::RW, c = i - r * G::RW;
             const int gy = ry0 + r, gx = rx0 + c;
             unsigned short v = 0;
             if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(fr + (size_t)gy * W + gx);
@@ -230,58 +342,37 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
         rowstart[tid] = 0x7fffffff;
         rowcount[tid] = 0;
     }
-    // offsets of the centroid circle (radius (d-1)/2, centers.wgsl order) and
-    // of the cpu_processed circle (radius d/2, kernels.rs order) in the row-pair
-    // layout, for an even (first half) and an odd (second half) base row
-    if (tid == 0) {
-        int k = 0;
-        const int rc = p.rint_c;
-        for (int i = -rc; i <= rc; ++i)
-            for (int j = -rc; j <= rc; ++j) {
-                const float x = (float)i, y = (float)j;
-                if (x * x + y * y > (float)rc * (float)rc) continue;
-                for (int e = 0; e < 2; ++e)
-                    ctoff[e * g.K1 + k] = ((((e + i) >> 1) * g.P2S + j) << 1) + ((e + i) & 1);
-                ctij[k] = make_float2(x, y);
-                ++k;
-            }
-    }
-    for (int k = tid; k < g.K2; k += FNT) {
-        const int i = __ldg(b.char_off + 2 * k), j = __ldg(b.char_off + 2 * k + 1);
-        for (int e = 0; e < 2; ++e) xtoff[e * g.K2 + k] = ((((e + i) >> 1) * g.P2S + j) << 1) + ((e + i) & 1);
-        xtab[k] = make_float4(__ldg(b.char_tab + 3 * k), __ldg(b.char_tab + 3 * k + 1),
-                              __ldg(b.char_tab + 3 * k + 2), 0.f);
-    }
+    if (p.cpu_processed)
+        for (int k = tid; k < G::K; k += FNT)
+            sc[k] = make_float2(__ldg(b.char_tab + 3 * k + 1), __ldg(b.char_tab + 3 * k + 2));
 
     // ---- 1. u16 -> f32 row pairs ----
-    const int RP = RH >> 1;
-    for (int i = tid; i < RP * RW; i += FNT) {
-        const int pr = fdiv16(i, g.mRW), c = i - pr * RW;
-        Rp[pr * g.RPS + c] = make_float2((float)U[(2 * pr) * RW + c], (float)U[(2 * pr + 1) * RW + c]);
+    for (int i = tid; i < G::RP * G::RW; i += FNT) {
+        const int pr = i / G::RW, c = i - pr * G::RW;
+        Rp[pr * G::RPS + c] = make_float2((float)U[(2 * pr) * G::RW + c], (float)U[(2 * pr + 1) * G::RW + c]);
     }
     __syncthreads();
 
     float2 W2[TAPS];
 #pragma unroll
     for (int j = 0; j < TAPS; ++j) W2[j] = make_float2(p.w[j], p.w[j]);
-    constexpr bool fd = true;  // the host verified the fixed-divisor division
 
     // ---- 2. row pass (preprocess_rows.wgsl) on row pairs ----
-    for (int it = tid; it < RP * g.NPW; it += FNT) {
-        const int q = fdiv16(it, g.mRP), pr = it - q * RP;
+    for (int it = tid; it < G::RP * G::NPW; it += FNT) {
+        const int q = it / G::RP, pr = it - q * G::RP;
         const int pc0 = q * FM;
-        const float2* src = Rp + pr * g.RPS + pc0;
+        const float2* src = Rp + pr * G::RPS + pc0;
         float2 v[FM + 2 * KR];
 #pragma unroll
         for (int i = 0; i < FM + 2 * KR; ++i) v[i] = src[i];
-        float2* gd = Gp + pr * g.GPS + pc0;
-        float2* bd = Bp + pr * g.GPS + pc0;
+        float2* gd = Gp + pr * G::GPS + pc0;
+        float2* bd = Bp + pr * G::GPS + pc0;
 #pragma unroll
         for (int m = 0; m < FM; ++m) {
             float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
             for (int j = 0; j < TAPS; ++j) acc = fma2(W2[j], v[m + j], acc);
-            gd[m] = fd ? div2(acc, g.dnorm) : make_float2(acc.x / p.norm, acc.y / p.norm);
+            gd[m] = div2(acc, dnorm);
         }
         const int fc0 = rx0 + pc0;  // frame column of v[0]
         if (fc0 >= 0 && fc0 + FM + 2 * KR - 1 < W) {
@@ -302,8 +393,8 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
                 float2 s = make_float2(0.f, 0.f);
 #pragma unroll
                 for (int j = 0; j < TAPS; ++j) {
-                    const int cc = clampi(reflect_once(fc - KR + j, W) - rx0, 0, RW - 1);
-                    s = add2(s, Rp[pr * g.RPS + cc]);
+                    const int cc = clampi(reflect_once(fc - KR + j, W) - rx0, 0, G::RW - 1);
+                    s = add2(s, Rp[pr * G::RPS + cc]);
                 }
                 bd[m] = s;
             }
@@ -313,12 +404,12 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
 
     // ---- 3. column pass (preprocess_cols.wgsl) -> P2 ----
     const float NEG = -CUDART_INF_F;
-    for (int it = tid; it < g.PWC * g.NRQ; it += FNT) {
-        const int rq = fdiv16(it, g.mPWC), c = it - rq * g.PWC;
+    for (int it = tid; it < G::PWC * G::NRQ; it += FNT) {
+        const int rq = it / G::PWC, c = it - rq * G::PWC;
         const int p0 = rq * (FM / 2);
         float2 L[FM / 2 + KR], ML[FM / 2 + KR - 1];
 #pragma unroll
-        for (int k = 0; k < FM / 2 + KR; ++k) L[k] = Gp[(p0 + k) * g.GPS + c];
+        for (int k = 0; k < FM / 2 + KR; ++k) L[k] = Gp[(p0 + k) * G::GPS + c];
 #pragma unroll
         for (int k = 0; k < FM / 2 + KR - 1; ++k) ML[k] = make_float2(L[k].y, L[k + 1].x);
         float2 gq[FM / 2];
@@ -327,13 +418,13 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
             float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
             for (int j = 0; j < TAPS; ++j) acc = fma2(W2[j], (j & 1) ? ML[m + (j >> 1)] : L[m + (j >> 1)], acc);
-            gq[m] = fd ? div2(acc, g.dnorm) : make_float2(acc.x / p.norm, acc.y / p.norm);
+            gq[m] = div2(acc, dnorm);
         }
         float2 cs[FM / 2];
         const int fr0 = ry0 + 2 * p0;  // frame row of raw row 2*p0
         if (fr0 >= 0 && fr0 + FM + 2 * KR - 1 < H) {
 #pragma unroll
-            for (int k = 0; k < FM / 2 + KR; ++k) L[k] = Bp[(p0 + k) * g.GPS + c];
+            for (int k = 0; k < FM / 2 + KR; ++k) L[k] = Bp[(p0 + k) * G::GPS + c];
 #pragma unroll
             for (int k = 0; k < FM / 2 + KR - 1; ++k) ML[k] = make_float2(L[k].y, L[k + 1].x);
 #pragma unroll
@@ -352,35 +443,39 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
                 const int fa = fr0 + 2 * m + KR;  // frame row of the output pair's first row
 #pragma unroll
                 for (int j = 0; j < TAPS; ++j) {
-                    const int ra = clampi(reflect_once(fa - KR + j, H) - ry0, 0, RH - 1);
-                    const int rb = clampi(reflect_once(fa + 1 - KR + j, H) - ry0, 0, RH - 1);
-                    sx = sx + Bf[(((ra >> 1) * g.GPS + c) << 1) + (ra & 1)];
-                    sy = sy + Bf[(((rb >> 1) * g.GPS + c) << 1) + (rb & 1)];
+                    const int ra = clampi(reflect_once(fa - KR + j, H) - ry0, 0, G::RH - 1);
+                    const int rb = clampi(reflect_once(fa + 1 - KR + j, H) - ry0, 0, G::RH - 1);
+                    sx = sx + Bf[(((ra >> 1) * G::GPS + c) << 1) + (ra & 1)];
+                    sy = sy + Bf[(((rb >> 1) * G::GPS + c) << 1) + (rb & 1)];
                 }
                 cs[m] = make_float2(sx, sy);
             }
         }
         const int fc = px0 + c;
-        const bool cin = fc >= 0 && fc < W && c < PW;
+        const bool cin = fc >= 0 && fc < W && c < G::PW;
+        const int fa0 = py0 + 2 * p0;  // frame row of the item's first output
+        const bool all_in = cin && fa0 >= 0 && fa0 + FM - 1 < H;
 #pragma unroll
         for (int m = 0; m < FM / 2; ++m) {
-            const float2 bq = fd ? div2(cs[m], g.dkk) : make_float2(cs[m].x / p.kk, cs[m].y / p.kk);
-            const float2 res = sub2(gq[m], bq);
-            const int fa = py0 + 2 * (p0 + m);
+            const float2 res = sub2(gq[m], div2(cs[m], dkk));
             float2 o;
-            o.x = (cin && fa >= 0 && fa < H) ? (res.x < 0.f ? 0.f : res.x) : NEG;
-            o.y = (cin && fa + 1 >= 0 && fa + 1 < H) ? (res.y < 0.f ? 0.f : res.y) : NEG;
-            P2[(p0 + m) * g.P2S + c] = o;
+            o.x = res.x < 0.f ? 0.f : res.x;  // preprocess_cols.wgsl:55-60
+            o.y = res.y < 0.f ? 0.f : res.y;
+            if (!all_in) {
+                const int fa = fa0 + 2 * m;
+                if (!(cin && fa >= 0 && fa < H)) o.x = NEG;
+                if (!(cin && fa + 1 >= 0 && fa + 1 < H)) o.y = NEG;
+            }
+            P2[(p0 + m) * G::P2S + c] = o;
         }
     }
     __syncthreads();
 
     // ---- 4. row max over the dilation window (max_rows.wgsl) ----
-    const int PP = PH >> 1;
-    for (int it = tid; it < PP * (FT / FM); it += FNT) {
-        const int q = fdiv16(it, g.mPP), pr = it - q * PP;
+    for (int it = tid; it < G::PP * (FT / FM); it += FNT) {
+        const int q = it / G::PP, pr = it - q * G::PP;
         const int tc0 = q * FM;
-        const float2* src = P2 + pr * g.P2S + tc0 + hx - O;
+        const float2* src = P2 + pr * G::P2S + tc0 + HX - O;
         float vx[FM + DD - 1], vy[FM + DD - 1];
 #pragma unroll
         for (int i = 0; i < FM + DD - 1; ++i) {
@@ -392,7 +487,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
         slide_max<DD, FM>(vx, ox);
         slide_max<DD, FM>(vy, oy);
 #pragma unroll
-        for (int m = 0; m < FM; ++m) RM2[pr * g.RMS + tc0 + m] = make_float2(ox[m], oy[m]);
+        for (int m = 0; m < FM; ++m) RM2[pr * G::RMS + tc0 + m] = make_float2(ox[m], oy[m]);
     }
     __syncthreads();
 
@@ -400,26 +495,27 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     for (int it = tid; it < FT * (TH0 / FM); it += FNT) {
         const int tc = it % FT, rq = it / FT;
         const int tr0 = rq * FM;
-        const int k0 = (tr0 + hp - O) >> 1;  // hp - O is even
+        const int k0 = (tr0 + HP - O) >> 1;  // HP - O is even
         constexpr int NPR = (FM + DD - 1 + 1) / 2;
-        float v[2 * NPR];
+        float vv[2 * NPR];
 #pragma unroll
         for (int k = 0; k < NPR; ++k) {
-            const float2 z = RM2[(k0 + k) * g.RMS + tc];
-            v[2 * k] = z.x;
-            v[2 * k + 1] = z.y;
+            const float2 z = RM2[(k0 + k) * G::RMS + tc];
+            vv[2 * k] = z.x;
+            vv[2 * k + 1] = z.y;
         }
-        float vv[FM + DD - 1];
+        float v[FM + DD - 1];
 #pragma unroll
-        for (int i = 0; i < FM + DD - 1; ++i) vv[i] = v[i];
+        for (int i = 0; i < FM + DD - 1; ++i) v[i] = vv[i];
         float cm[FM];
-        slide_max<DD, FM>(vv, cm);
+        slide_max<DD, FM>(v, cm);
         const float* Pf = (const float*)P2;
+        const bool col_in = tx0 + tc < W;
 #pragma unroll
         for (int m = 0; m < FM; ++m) {
-            const int r = tr0 + m + hp;  // processed row of the centre
-            const float center = Pf[(((r >> 1) * g.P2S + tc + hx) << 1) + (r & 1)];
-            const bool in = tr0 + m < TH && tx0 + tc < W;
+            const int r = tr0 + m + HP;  // processed row of the centre
+            const float center = Pf[(((r >> 1) * G::P2S + tc + HX) << 1) + (r & 1)];
+            const bool in = col_in && tr0 + m < TH;
             const bool f = in && cm[m] <= center && !(p.zero_skip && center == 0.f);
             flags[(tr0 + m) * FT + tc] = f ? 1 : 0;
         }
@@ -427,26 +523,29 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     __syncthreads();
 
     // ---- 6. raster-order compaction, walks, emission ----
-    const int npx = TH0 * FT;
-    const int chunk = npx / FNT;  // 8 or 16 flags per thread
-    const int q0 = tid * chunk;
+    constexpr int CHUNK = TH0 * FT / FNT;  // 8 or 16 flags per thread
+    const int q0 = tid * CHUNK;
     int mine = 0;
-    for (int i = 0; i < chunk; ++i) mine += flags[q0 + i];
+    unsigned char fl[CHUNK];
+#pragma unroll
+    for (int i = 0; i < CHUNK; ++i) {
+        fl[i] = flags[q0 + i];
+        mine += fl[i];
+    }
     int pos = block_excl_scan<FNT>(mine, warp_tot, &s_total);
     const int ncand = s_total;
-    for (int q = q0; q < q0 + chunk; ++q)
-        if (flags[q]) clist[pos++] = q;
+#pragma unroll
+    for (int i = 0; i < CHUNK; ++i)
+        if (fl[i]) clist[pos++] = q0 + i;
     __syncthreads();
 
-    P2Acc acc{(const float*)P2, py0, px0, PH, PW, g.P2S};
+    P2Acc<G> acc{(const float*)P2, py0, px0};
     const unsigned short* frame = (const unsigned short*)b.frames + (size_t)t * H * W;
     GRawAcc racc{frame, W};
-    // thread k serves candidate (k % 32) * 8 + k / 32: one lane per warp first
-    const int cidx = (tid & 31) * (FNT / 32) + (tid >> 5);
     int emitted = 0;
     for (int r0 = 0; r0 < ncand; r0 += FCMAX) {
         const int nr = min(FCMAX, ncand - r0);
-        for (int c = cidx; c < nr; c += FNT) {
+        for (int c = tid; c < nr; c += FNT) {
             const int q = clist[r0 + c];
             const int u0 = ty0 + q / FT, v0 = tx0 + q % FT;
             int st;
@@ -459,7 +558,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
                 float c0 = 0.f, c1 = 0.f;
                 bool ok = true;
                 for (int iter = 0; iter < p.max_iter; ++iter) {
-                    if (!centroid_tab(p, acc, ctoff, ctij, g.K1, u, v, c0, c1, m)) { ok = false; break; }
+                    if (!centroid_fixed<G, RC>(p, acc, u, v, c0, c1, m)) { ok = false; break; }
                     bool changed = false;
                     if (c0 > p.thr && u < H - 1) { u += 1; changed = true; }
                     else if (c0 < -p.thr && u > 0) { u -= 1; changed = true; }
@@ -517,42 +616,14 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
             rec.g_rg = rec.g_raw = rec.g_sig = rec.g_ecc = 0.f;
             rec.pad = 0.f;
             if (p.cpu_processed) {
-                // execute_gpu.rs:286-299: products summed per ndarray's
-                // eight-accumulator fold, all three sums in one pass
+                // execute_gpu.rs:165-172, 286-299 at the originating pixel
                 const int rr = u0 - py0, cc = v0 - px0;
-                const int base2 = (((rr >> 1) * g.P2S + cc) << 1);
-                const int* T = xtoff + (rr & 1) * g.K2;
-                const float* Pf = (const float*)P2;
-                float ar[8], as[8], ac[8];
-#pragma unroll
-                for (int l = 0; l < 8; ++l) { ar[l] = 0.f; as[l] = 0.f; ac[l] = 0.f; }
-                const int K = g.K2, K8 = K & ~7;
-                float sig = Pf[base2 + T[0]];
-                for (int k0 = 0; k0 < K8; k0 += 8) {
-#pragma unroll
-                    for (int l = 0; l < 8; ++l) {
-                        const float nb = Pf[base2 + T[k0 + l]];
-                        const float4 tb = xtab[k0 + l];
-                        ar[l] = ar[l] + nb * tb.x;
-                        as[l] = as[l] + nb * tb.y;
-                        ac[l] = ac[l] + nb * tb.z;
-                        sig = fmaxf(sig, nb);
-                    }
-                }
-                float rg = 0.f, sn = 0.f, cs = 0.f;
-                rg = rg + (ar[0] + ar[4]); rg = rg + (ar[1] + ar[5]); rg = rg + (ar[2] + ar[6]); rg = rg + (ar[3] + ar[7]);
-                sn = sn + (as[0] + as[4]); sn = sn + (as[1] + as[5]); sn = sn + (as[2] + as[6]); sn = sn + (as[3] + as[7]);
-                cs = cs + (ac[0] + ac[4]); cs = cs + (ac[1] + ac[5]); cs = cs + (ac[2] + ac[6]); cs = cs + (ac[3] + ac[7]);
-                for (int k = K8; k < K; ++k) {
-                    const float nb = Pf[base2 + T[k]];
-                    const float4 tb = xtab[k];
-                    rg = rg + nb * tb.x;
-                    sn = sn + nb * tb.y;
-                    cs = cs + nb * tb.z;
-                    sig = fmaxf(sig, nb);
-                }
+                const int base2 = (((rr >> 1) * G::P2S + cc) << 1);
+                float rg, sn, cs2, sig;
+                if (rr & 1) circle_features<RC, 1, G::P2S>((const float*)P2, base2, sc, rg, sn, cs2, sig);
+                else circle_features<RC, 0, G::P2S>((const float*)P2, base2, sc, rg, sn, cs2, sig);
                 rec.rg_sum = rg;
-                rec.eccn = sqrtf(sn * sn + cs * cs);
+                rec.eccn = sqrtf(sn * sn + cs2 * cs2);
                 rec.mid = acc(u0, v0);
                 rec.signal = sig;
             }
@@ -592,37 +663,72 @@ __global__ void verify_division_kernel(float divisor, FixedDiv f, unsigned int* 
     if (bad) atomicAdd(mismatches, bad);
 }
 
-// (smoothing radius, dilation size) pairs with a specialised kernel; other
-// parameter sets use locate_tiles_kernel.  Covers diameters 5-11 with the
-// default separation (diameter + 1) and smoothing (diameter).
-#define GT_FAST_LIST(X) X(2, 8) X(3, 11) X(4, 14) X(5, 16) X(2, 11) X(3, 8) X(4, 11) X(3, 14)
+namespace {
+// TMA descriptor over the movie (u16, dims W x H x T) with a box of the raw
+// tile.  Needs a 16-byte aligned base and a row pitch multiple of 16 bytes.
+bool make_tensor_map(CUtensorMap* map, const void* frames, int T, int H, int W, int box_w, int box_h) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    if (((uintptr_t)frames & 15) || (W * 2) % 16) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)T};
+    cuuint64_t strides[2] = {(cuuint64_t)W * 2, (cuuint64_t)W * H * 2};
+    cuuint32_t box[3] = {(cuuint32_t)box_w, (cuuint32_t)box_h, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, const_cast<void*>(frames), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+}  // namespace
 
-bool fast_supported(int kr, int dd) {
-#define GT_FAST_CASE(KR, DD) if (kr == KR && dd == DD) return true;
+// (smoothing radius, dilation size, centroid radius) triples with a
+// specialised kernel: diameters 5, 7, 9, 11 (odd, centroid radius
+// (d - 1) / 2) with the default smoothing (= diameter) and separation
+// (= diameter + 1), plus neighbouring separations.  Everything else uses
+// locate_tiles_kernel.
+#define GT_FAST_LIST(X) X(2, 8, 2) X(3, 11, 3) X(4, 14, 4) X(5, 16, 5) X(3, 8, 3) X(4, 11, 4) X(2, 7, 2) X(3, 12, 3)
+
+bool fast_supported(int kr, int dd, int rc, int diameter) {
+    if (diameter != 2 * rc + 1) return false;
+#define GT_FAST_CASE(KR, DD, RC) if (kr == KR && dd == DD && rc == RC) return true;
     GT_FAST_LIST(GT_FAST_CASE)
 #undef GT_FAST_CASE
     return false;
 }
 
-cudaError_t launch_locate_fast(int kr, int dd, int th, dim3 grid, cudaStream_t st, const LocParams& p,
-                               const MovieBufs& b, const FastGeo& g, const CUtensorMap& map, int frame0) {
-#define GT_FAST_CASE(KR, DD)                                                                          \
-    if (kr == KR && dd == DD) {                                                                       \
-        if (th == 32) {                                                                               \
-            cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD, 32>,                       \
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, g.smem); \
-            if (e != cudaSuccess) return e;                                                           \
-            locate_fast_kernel<KR, DD, 32><<<grid, FNT, g.smem, st>>>(p, b, g, map, frame0);           \
-        } else {                                                                                      \
-            cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD, 64>,                       \
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, g.smem); \
-            if (e != cudaSuccess) return e;                                                           \
-            locate_fast_kernel<KR, DD, 64><<<grid, FNT, g.smem, st>>>(p, b, g, map, frame0);           \
-        }                                                                                             \
-        return cudaGetLastError();                                                                    \
+// Launches the specialised kernel over frames [frame0, frame0 + grid.y).
+// *used_tma reports whether the raw tiles were staged by TMA.
+cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaStream_t st, const LocParams& p,
+                               const MovieBufs& b, FixedDiv dnorm, FixedDiv dkk, int T, int frame0,
+                               int* used_tma) {
+#define GT_FAST_LAUNCH(KR, DD, RC, TH)                                                                  \
+    {                                                                                                   \
+        using G = Geo<KR, DD, TH, RC>;                                                                  \
+        CUtensorMap map;                                                                                \
+        std::memset(&map, 0, sizeof(map));                                                              \
+        const int tma = make_tensor_map(&map, b.frames, T, p.H, p.W, G::RW, G::RH) ? 1 : 0;            \
+        *used_tma = tma;                                                                                \
+        cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD, TH, RC>,                         \
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);      \
+        if (e != cudaSuccess) return e;                                                                 \
+        locate_fast_kernel<KR, DD, TH, RC><<<grid, FNT, G::SMEM, st>>>(p, b, dnorm, dkk, map, tma, frame0); \
+        return cudaGetLastError();                                                                      \
+    }
+#define GT_FAST_CASE(KR, DD, RC)                                                                        \
+    if (kr == KR && dd == DD && rc == RC) {                                                             \
+        if (th == 32) GT_FAST_LAUNCH(KR, DD, RC, 32)                                                    \
+        else GT_FAST_LAUNCH(KR, DD, RC, 64)                                                             \
     }
     GT_FAST_LIST(GT_FAST_CASE)
 #undef GT_FAST_CASE
+#undef GT_FAST_LAUNCH
     return cudaErrorInvalidValue;
 }
 
