@@ -150,6 +150,8 @@ typedef struct gt_stats {
     float ms_assemble;         /* output table */
     float ms_total;            /* first to last kernel of the call */
     int32_t locate_kernel;     /* 0 generic, 1 specialised, 2 specialised with TMA staging */
+    float link_phase_ms[4];    /* linker: first pass, roots, memory entries, relinking */
+    int32_t link_dirty[8];     /* frames relinked by fixed-point passes 1..8 */
 } gt_stats;
 
 GT_API int gt_last_stats(const gt_ctx* ctx, gt_stats* out);

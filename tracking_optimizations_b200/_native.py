@@ -74,6 +74,8 @@ class GtStats(ctypes.Structure):
         ("ms_assemble", ctypes.c_float),
         ("ms_total", ctypes.c_float),
         ("locate_kernel", ctypes.c_int32),
+        ("link_phase_ms", ctypes.c_float * 4),
+        ("link_dirty", ctypes.c_int32 * 8),
     ]
 
 
@@ -159,7 +161,10 @@ def set_option(key, value, device=0):
 def last_stats(device=0):
     s = GtStats()
     load().gt_last_stats(context(device), ctypes.byref(s))
-    return {k: getattr(s, k) for k, _ in GtStats._fields_}
+    out = {k: getattr(s, k) for k, _ in GtStats._fields_}
+    out["link_phase_ms"] = list(out["link_phase_ms"])
+    out["link_dirty"] = list(out["link_dirty"])
+    return out
 
 
 def make_params(diameter, **kw):

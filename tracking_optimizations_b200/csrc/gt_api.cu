@@ -22,10 +22,8 @@ namespace gt {
 __global__ void locate_tiles_kernel(const LocParams p, const MovieBufs b, int frame0);
 __global__ void fallback_walk_kernel(const LocParams p, const MovieBufs b, int win);
 __global__ void finalize_kernel(const LocParams p, MovieBufs b, float sep, int link_grid);
-__global__ void link_frames_kernel(LinkBufs L, int only_dirty);
-__global__ void memory_kernel(LinkBufs L, int memory);
-__global__ void root_init_kernel(LinkBufs L, const int* total);
-__global__ void root_jump_kernel(LinkBufs L, const int* total);
+__global__ void link_fixpoint_kernel(LinkBufs L, int memory, int max_passes, int rounds, int* ndirty,
+                                     int* passes, unsigned long long* phase_ns);
 __global__ void scan_frames_kernel(const int* in, int* out, int n);
 __global__ void newid_kernel(const int* newrank, const int* newbase, const int* off, const int* npart,
                              int* newid, int T);
@@ -321,6 +319,7 @@ struct Work {
     int *char_off, *sig_off, *bg_off;
     int* err;
     int *off, *pred, *mlist, *mcount, *dirty, *ndirty, *newrank, *newcount, *newbase, *root, *newid;
+    unsigned long long* phase_ns;
     unsigned char* lnext;
     float *s_y, *s_x, *e_w, *d_w;
     int *s_h, *s_deg, *e_dst, *d_cnt, *d_src, *uf, *c_nd, *c_ns, *c_min, *work, *bump, *hkey, *hval;
@@ -379,7 +378,8 @@ size_t carve(const Plan& P, char* base, Work* w, size_t frame_bytes, bool need_l
     w->mlist = c.take<int>(P.link ? T * P.cap_m : 1);
     w->mcount = c.take<int>(T);
     w->dirty = c.take<int>(T);
-    w->ndirty = c.take<int>(1);
+    w->ndirty = c.take<int>(T + 2);
+    w->phase_ns = c.take<unsigned long long>(4);
     w->newrank = c.take<int>(np);
     w->newcount = c.take<int>(T);
     w->newbase = c.take<int>(T + 1);
@@ -445,51 +445,35 @@ LinkBufs link_bufs(const Plan& P, const Work& w) {
 }
 
 // Linking over the particle tables already in the workspace (npart, py, px,
-// gstart/gidx, off).  Leaves trajectory ids in newid[root[g]].
+// gstart/gidx, off): one cooperative launch runs the whole fixed point
+// (link_fixpoint_kernel), then new trajectory ids are numbered.  Leaves the
+// trajectory id of particle g in newid[root[g]].
 int run_link(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
     LinkBufs L = link_bufs(P, w);
-    const int T = P.T;
+    int T = P.T;
     CK(cudaMemsetAsync(w.mcount, 0, sizeof(int) * T, st));
     CK(cudaMemsetAsync(w.dirty, 0, sizeof(int) * T, st));
-    link_frames_kernel<<<P.nslot, 256, 0, st>>>(L, 0);
-    CK(cudaGetLastError());
-    ctx->stats.launches += 1;
+    CK(cudaMemsetAsync(w.ndirty, 0, sizeof(int) * (T + 2), st));
     int rounds = 1;
     while ((1 << rounds) < T + 1) ++rounds;
     rounds += 1;
-    const int rblocks = ctx->num_sms * 8;
-    auto roots = [&]() -> int {
-        root_init_kernel<<<rblocks, 256, 0, st>>>(L, w.off + T);
-        for (int i = 0; i < rounds; ++i) root_jump_kernel<<<rblocks, 256, 0, st>>>(L, w.off + T);
-        CK(cudaGetLastError());
-        ctx->stats.launches += 1 + rounds;
-        return GT_OK;
-    };
-    int iters = 0;
-    if (P.r.memory > 0 && T > 2) {
-        for (iters = 1; iters <= T + 1; ++iters) {
-            int rc = roots();
-            if (rc) return rc;
-            CK(cudaMemsetAsync(w.ndirty, 0, sizeof(int), st));
-            memory_kernel<<<P.nslot, 256, 0, st>>>(L, (int)P.r.memory);
-            CK(cudaGetLastError());
-            ctx->stats.launches += 1;
-            int nd = 0;
-            CK(cudaMemcpyAsync(&nd, w.ndirty, sizeof(int), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            if (nd == 0) break;
-            link_frames_kernel<<<P.nslot, 256, 0, st>>>(L, 1);
-            CK(cudaGetLastError());
-            ctx->stats.launches += 1;
-        }
-    }
-    ctx->stats.link_iterations = iters;
-    int rc = roots();
-    if (rc) return rc;
+    L.lsm_bytes = 96 * 1024;
+    CK(cudaFuncSetAttribute(link_fixpoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.lsm_bytes));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_kernel, 256, L.lsm_bytes));
+    const int grid = std::max(1, std::min(P.nslot, per_sm * ctx->num_sms));
+    int memory = (int)P.r.memory;
+    int max_passes = T + 1;
+    int* ndirty = w.ndirty;
+    int* passes = w.err + 1;
+    unsigned long long* phase_ns = w.phase_ns;
+    void* args[] = {&L, &memory, &max_passes, &rounds, &ndirty, &passes, &phase_ns};
+    CK(cudaLaunchCooperativeKernel((const void*)link_fixpoint_kernel, dim3(grid), dim3(256), args, L.lsm_bytes,
+                                   st));
     scan_frames_kernel<<<1, 1024, 0, st>>>(w.newcount, w.newbase, T);
     newid_kernel<<<T, 256, 0, st>>>(w.newrank, w.newbase, w.off, w.npart, w.newid, T);
     CK(cudaGetLastError());
-    ctx->stats.launches += 2;
+    ctx->stats.launches += 3;
     return GT_OK;
 }
 
@@ -643,6 +627,15 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
     }
     *err_bits = hb[0];
     *nrows = hb[4];
+    ctx->stats.link_iterations = P.link ? hb[1] : 0;
+    if (P.link) {
+        unsigned long long ph[4];
+        CK(cudaMemcpy(ph, w.phase_ns, sizeof(ph), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < 4; ++i) ctx->stats.link_phase_ms[i] = (float)(ph[i] * 1e-6);
+        int nd[9] = {0};
+        CK(cudaMemcpy(nd, w.ndirty, sizeof(int) * std::min(9, T + 2), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < 8; ++i) ctx->stats.link_dirty[i] = i + 1 < T + 2 ? nd[i + 1] : 0;
+    }
     ctx->stats.fallback_walks = np;
     ctx->stats.particles = hb[4];
     ctx->stats.candidates = nc_total;

@@ -148,6 +148,7 @@ struct LinkBufs {
     int* hkey;            // hash tables, hsize per slot
     int* hval;
     int hsize;
+    int lsm_bytes;        // dynamic shared memory pool of the linker blocks
 };
 
 struct AsmArgs {

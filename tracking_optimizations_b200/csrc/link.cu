@@ -15,7 +15,11 @@
 // only frames whose M changed are linked again, until M is a fixed point.
 // M(t) depends on frames < t only, so iteration k settles frame k at the
 // latest and the fixed point is the sequential result.
+#include <cooperative_groups.h>
+
 #include "gt_device.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace gt {
 
@@ -78,7 +82,7 @@ __device__ int block_scan_inplace_l(int* data, int n, int* warp_tot, int* s_tota
 // dests: destination indices in DFS order; sources are chosen through the
 // per-destination lists d_src/d_w (ascending source index); null costs r^2.
 // Returns false when the option-trial budget is exhausted.
-__device__ bool solve_subnet(const LinkBufs& L, int slot, const int* dests, int nd, const int* d_off,
+__device__ bool solve_subnet(const LinkBufs& L, const int* dests, int nd, const int* d_off,
                              const int* d_src, const float* d_w, unsigned char* used, int* oi,
                              int* cur, int* best_choice, float null_cost) {
     float score = 0.f, best = CUDART_INF_F;
@@ -136,34 +140,21 @@ __device__ bool solve_subnet(const LinkBufs& L, int slot, const int* dests, int 
 }  // namespace
 
 // One CTA per frame (grid-stride); frame t >= 1 links P(t-1) + M(t) to P(t).
-__global__ void __launch_bounds__(NTL) link_frames_kernel(LinkBufs L, int only_dirty) {
+__device__ void link_frames_body(const LinkBufs& L, int only_dirty) {
     __shared__ int warp_tot[NTL / 32];
     __shared__ int s_total;
+    __shared__ int s_bump;
+    extern __shared__ __align__(16) int lsm[];  // per-frame scratch pool
     const int slot = blockIdx.x;
     const int cap_s = L.cap_s, cap_p = L.cap_p;
-    float* sy = L.s_y + (size_t)slot * cap_s;
-    float* sx = L.s_x + (size_t)slot * cap_s;
-    int* sh = L.s_h + (size_t)slot * cap_s;
-    int* sdeg = L.s_deg + (size_t)slot * (cap_s + 1);
-    int* edst = L.e_dst + (size_t)slot * L.cap_e;
-    float* ew = L.e_w + (size_t)slot * L.cap_e;
-    int* dcnt = L.d_cnt + (size_t)slot * (cap_p + 1);
-    int* dsrc = L.d_src + (size_t)slot * L.cap_e;
-    float* dw = L.d_w + (size_t)slot * L.cap_e;
     const int nn = cap_s + cap_p;
-    int* uf = L.uf + (size_t)slot * nn;
-    int* cnd = L.c_nd + (size_t)slot * nn;
-    int* cns = L.c_ns + (size_t)slot * nn;
-    int* cmin = L.c_min + (size_t)slot * nn;
-    unsigned char* vis = L.vis + (size_t)slot * nn;
-    int* work = L.work + (size_t)slot * 4 * nn;
-    int* bump = L.bump + slot;
     const float r = L.r;
     const float G = (float)L.G;
     const int ncell = L.ncx * L.ncy;
+    const int pool = L.lsm_bytes / 4;
 
     for (int t = blockIdx.x; t < L.T; t += gridDim.x) {
-        if (only_dirty && !L.dirty[t]) continue;
+        if (only_dirty && !__ldcg(L.dirty + t)) continue;
         const int nd = L.npart[t];
         int* pred = L.pred + L.off[t];
         if (t == 0) {
@@ -171,24 +162,69 @@ __global__ void __launch_bounds__(NTL) link_frames_kernel(LinkBufs L, int only_d
             __syncthreads();
         } else {
             const int n1 = L.npart[t - 1];
-            const int nm = L.mcount[t];
+            const int nm = __ldcg(L.mcount + t);
             const int ns = n1 + nm;
+            const int nnode = ns + nd;
+            // the frame's particles, grid and scratch live in shared memory
+            // when they fit (latency), else in this block's global slot
+            const int need = 3 * nd + ncell + 1 + 4 * ns + 1 + nd + 1 + 8 * nnode + (nnode + 3) / 4;
+            const bool sm = need <= pool;
+            int* o = lsm;
+            auto take = [&](int n) { int* q = o; o += n; return q; };
+            const float* dy;
+            const float* dx;
+            const int* gs;
+            const int* gi;
+            float *sy, *sx;
+            int *sh, *sdeg, *dcnt, *uf, *cnd, *cns, *cmin, *work;
+            unsigned char* vis;
+            if (sm) {
+                float* ddy = (float*)take(nd);
+                float* ddx = (float*)take(nd);
+                int* ggs = take(ncell + 1);
+                int* ggi = take(nd);
+                const float* py_t = L.py + (size_t)t * cap_p;
+                const float* px_t = L.px + (size_t)t * cap_p;
+                const int* gs_t = L.gstart + (size_t)t * (ncell + 1);
+                const int* gi_t = L.gidx + (size_t)t * cap_p;
+                for (int i = threadIdx.x; i < nd; i += NTL) { ddy[i] = py_t[i]; ddx[i] = px_t[i]; ggi[i] = gi_t[i]; }
+                for (int i = threadIdx.x; i <= ncell; i += NTL) ggs[i] = gs_t[i];
+                dy = ddy; dx = ddx; gs = ggs; gi = ggi;
+                sy = (float*)take(ns); sx = (float*)take(ns); sh = take(ns); sdeg = take(ns + 1);
+                dcnt = take(nd + 1);
+                uf = take(nnode); cnd = take(nnode); cns = take(nnode); cmin = take(nnode);
+                work = take(4 * nnode);
+                vis = (unsigned char*)take((nnode + 3) / 4);
+            } else {
+                dy = L.py + (size_t)t * cap_p;
+                dx = L.px + (size_t)t * cap_p;
+                gs = L.gstart + (size_t)t * (ncell + 1);
+                gi = L.gidx + (size_t)t * cap_p;
+                sy = L.s_y + (size_t)slot * cap_s;
+                sx = L.s_x + (size_t)slot * cap_s;
+                sh = L.s_h + (size_t)slot * cap_s;
+                sdeg = L.s_deg + (size_t)slot * (cap_s + 1);
+                dcnt = L.d_cnt + (size_t)slot * (cap_p + 1);
+                uf = L.uf + (size_t)slot * nn;
+                cnd = L.c_nd + (size_t)slot * nn;
+                cns = L.c_ns + (size_t)slot * nn;
+                cmin = L.c_min + (size_t)slot * nn;
+                vis = L.vis + (size_t)slot * nn;
+                work = L.work + (size_t)slot * 4 * nn;
+            }
+            int* bump = &s_bump;
             if (threadIdx.x == 0) *bump = 0;
             // sources: P(t-1) then M(t) (linking.rs:244-259 order)
             for (int s = threadIdx.x; s < ns; s += NTL) {
                 int h;
                 if (s < n1) h = (t - 1) * cap_p + s;
-                else h = L.mlist[(size_t)t * L.cap_m + (s - n1)];
+                else h = __ldcg(L.mlist + (size_t)t * L.cap_m + (s - n1));
                 sh[s] = h;
                 sy[s] = L.py[h];
                 sx[s] = L.px[h];
             }
             for (int s = threadIdx.x; s < n1; s += NTL) L.lnext[(size_t)(t - 1) * cap_p + s] = 0;
             __syncthreads();
-            const int* gs = L.gstart + (size_t)t * (ncell + 1);
-            const int* gi = L.gidx + (size_t)t * cap_p;
-            const float* dy = L.py + (size_t)t * cap_p;
-            const float* dx = L.px + (size_t)t * cap_p;
             // candidate pairs: degree pass
             for (int s = threadIdx.x; s < ns; s += NTL) {
                 const float qy = sy[s], qx = sx[s];
@@ -214,6 +250,16 @@ __global__ void __launch_bounds__(NTL) link_frames_kernel(LinkBufs L, int only_d
             __syncthreads();
             const int ne = block_scan_inplace_l(sdeg, ns, warp_tot, &s_total);
             if (threadIdx.x == 0) sdeg[ns] = ne;
+            int *edst, *dsrc;
+            float *ew, *dw;
+            if (sm && need + 4 * ne <= pool) {
+                edst = take(ne); ew = (float*)take(ne); dsrc = take(ne); dw = (float*)take(ne);
+            } else {
+                edst = L.e_dst + (size_t)slot * L.cap_e;
+                ew = L.e_w + (size_t)slot * L.cap_e;
+                dsrc = L.d_src + (size_t)slot * L.cap_e;
+                dw = L.d_w + (size_t)slot * L.cap_e;
+            }
             if (ne > L.cap_e) {
                 if (threadIdx.x == 0) atomicOr(L.err, ERR_EDGE_OVERFLOW);
                 for (int i = threadIdx.x; i < nd; i += NTL) pred[i] = -1;
@@ -275,7 +321,6 @@ __global__ void __launch_bounds__(NTL) link_frames_kernel(LinkBufs L, int only_d
                 }
             }
             // union-find over sources [0, ns) and destinations [ns, ns + nd)
-            const int nnode = ns + nd;
             for (int i = threadIdx.x; i < nnode; i += NTL) {
                 uf[i] = i; cnd[i] = 0; cns[i] = 0; vis[i] = 0;
             }
@@ -347,8 +392,7 @@ __global__ void __launch_bounds__(NTL) link_frames_kernel(LinkBufs L, int only_d
                 int* cur = stk_p;
                 int* bestc = choice;
                 for (int q = 0; q < npath; ++q) bestc[q] = -1;
-                const bool ok = solve_subnet(L, slot, path, npath, dcnt, dsrc, dw, vis, oi, cur, bestc,
-                                             null_cost);
+                const bool ok = solve_subnet(L, path, npath, dcnt, dsrc, dw, vis, oi, cur, bestc, null_cost);
                 if (!ok) atomicOr(L.err, ERR_SUBNET_BUDGET);
                 for (int q = 0; q < npath; ++q) {
                     const int s = bestc[q];
@@ -378,47 +422,76 @@ __global__ void __launch_bounds__(NTL) link_frames_kernel(LinkBufs L, int only_d
 // linking.rs:479-485, oldest list first, index order within a list),
 // skipping trajectories present in frame t-1 and keeping the first entry of
 // each trajectory.  Marks frames whose M changed.
-__global__ void __launch_bounds__(NTL) memory_kernel(LinkBufs L, int memory) {
+__device__ void memory_body(const LinkBufs& L, int memory, int* ndirty) {
     __shared__ int warp_tot[NTL / 32];
     __shared__ int s_total;
     __shared__ int s_diff;
+    __shared__ int s_red;
+    extern __shared__ __align__(16) int lsm[];
     const int slot = blockIdx.x;
     const int cap_p = L.cap_p;
     const int nn = L.cap_s + cap_p;
-    int* ch = L.work + (size_t)slot * 4 * nn;    // candidate slab handles
-    int* cr = ch + nn;                            // candidate roots
-    int* cpos = cr + nn;                          // scan workspace
-    int* hk = L.hkey + (size_t)slot * L.hsize;
-    int* hv = L.hval + (size_t)slot * L.hsize;
+    const int pool = L.lsm_bytes / 4;
     for (int t = blockIdx.x; t < L.T; t += gridDim.x) {
         const int fbeg = max(0, t - 1 - memory), fend = t - 2;
         if (fend < fbeg) continue;
+        // number of candidates, to place the scratch
+        if (threadIdx.x == 0) s_red = 0;
+        __syncthreads();
+        {
+            int cnt = 0;
+            for (int f = fbeg; f <= fend; ++f) {
+                const int n = L.npart[f];
+                const unsigned char* ln = L.lnext + (size_t)f * cap_p;
+                for (int i = threadIdx.x; i < n; i += NTL) cnt += __ldcg(ln + i) ? 0 : 1;
+            }
+            atomicAdd(&s_red, cnt);
+        }
+        __syncthreads();
+        const int ncnt = s_red;
+        const int n1 = L.npart[t - 1];
+        int hs1 = 64;
+        while (hs1 < 2 * n1) hs1 <<= 1;
+        int hs2 = 64;
+        while (hs2 < 2 * ncnt) hs2 <<= 1;
+        int nmax = 0;
+        for (int f = fbeg; f <= fend; ++f) nmax = max(nmax, L.npart[f]);
+        const int cn = max(ncnt, nmax) + 1;
+        const bool sm = 3 * cn + 2 * (hs1 + hs2) <= pool;
+        int *ch, *cr, *cpos, *hk, *hv;
+        int lim;
+        if (sm) {
+            ch = lsm; cr = ch + cn; cpos = cr + cn; hk = cpos + cn; hv = hk + hs1 + hs2;
+            lim = cn;
+        } else {
+            ch = L.work + (size_t)slot * 4 * nn;
+            cr = ch + nn;
+            cpos = cr + nn;
+            hk = L.hkey + (size_t)slot * L.hsize;
+            hv = L.hval + (size_t)slot * L.hsize;
+            lim = nn;
+        }
         // candidates in (frame, index) order
         int nc = 0;
         for (int f = fbeg; f <= fend; ++f) {
             const int n = L.npart[f];
             const unsigned char* ln = L.lnext + (size_t)f * cap_p;
-            for (int i = threadIdx.x; i < n; i += NTL) cpos[i] = ln[i] ? 0 : 1;
+            for (int i = threadIdx.x; i < n; i += NTL) cpos[i] = __ldcg(ln + i) ? 0 : 1;
             __syncthreads();
             const int k = block_scan_inplace_l(cpos, n, warp_tot, &s_total);
             for (int i = threadIdx.x; i < n; i += NTL) {
-                if (ln[i]) continue;
+                if (__ldcg(ln + i)) continue;
                 const int j = nc + cpos[i];
-                if (j < nn) {
+                if (j < lim) {
                     ch[j] = f * cap_p + i;
-                    cr[j] = L.root[L.off[f] + i];
+                    cr[j] = __ldcg(L.root + L.off[f] + i);
                 }
             }
             nc += k;
             __syncthreads();
         }
-        if (nc > nn) { if (threadIdx.x == 0) atomicOr(L.err, ERR_MEM_OVERFLOW); nc = nn; }
-        const int n1 = L.npart[t - 1];
-        int hs1 = 64;
-        while (hs1 < 2 * n1) hs1 <<= 1;
-        int hs2 = 64;
-        while (hs2 < 2 * nc) hs2 <<= 1;
-        if (hs1 + hs2 > L.hsize) { if (threadIdx.x == 0) atomicOr(L.err, ERR_SCRATCH_OVERFLOW); continue; }
+        if (nc > lim) { if (threadIdx.x == 0) atomicOr(L.err, ERR_MEM_OVERFLOW); nc = lim; }
+        if (!sm && hs1 + hs2 > L.hsize) { if (threadIdx.x == 0) atomicOr(L.err, ERR_SCRATCH_OVERFLOW); continue; }
         int* k1 = hk;
         int* k2 = hk + hs1;
         int* v2 = hv + hs1;
@@ -426,7 +499,7 @@ __global__ void __launch_bounds__(NTL) memory_kernel(LinkBufs L, int memory) {
         __syncthreads();
         // trajectories present in frame t-1
         for (int i = threadIdx.x; i < n1; i += NTL) {
-            const int key = L.root[L.off[t - 1] + i];
+            const int key = __ldcg(L.root + L.off[t - 1] + i);
             unsigned hsh = ((unsigned)key * 2654435761u) & (hs1 - 1);
             while (true) {
                 const int prev = atomicCAS(&k1[hsh], -1, key);
@@ -467,14 +540,14 @@ __global__ void __launch_bounds__(NTL) memory_kernel(LinkBufs L, int memory) {
         __syncthreads();
         const int nk = block_scan_inplace_l(cpos, nc, warp_tot, &s_total);
         int* ml = L.mlist + (size_t)t * L.cap_m;
-        const int old = L.mcount[t];
+        const int old = __ldcg(L.mcount + t);
         if (nk > L.cap_m) { if (threadIdx.x == 0) atomicOr(L.err, ERR_MEM_OVERFLOW); continue; }
         if (old != nk && threadIdx.x == 0) s_diff = 1;
         __syncthreads();
         for (int j = threadIdx.x; j < nc; j += NTL) {
             const int a = cpos[j];
             const int nxt = (j + 1 < nc) ? cpos[j + 1] : nk;
-            if (nxt > a && ml[a] != ch[j]) s_diff = 1;
+            if (nxt > a && __ldcg(ml + a) != ch[j]) s_diff = 1;
         }
         __syncthreads();
         if (s_diff) {
@@ -486,7 +559,7 @@ __global__ void __launch_bounds__(NTL) memory_kernel(LinkBufs L, int memory) {
             if (threadIdx.x == 0) {
                 L.mcount[t] = nk;
                 L.dirty[t] = 1;
-                atomicAdd(L.ndirty, 1);
+                atomicAdd(ndirty, 1);
             }
         } else if (threadIdx.x == 0) {
             L.dirty[t] = 0;
@@ -495,19 +568,78 @@ __global__ void __launch_bounds__(NTL) memory_kernel(LinkBufs L, int memory) {
     }
 }
 
-// Trajectory roots by pointer jumping over `pred` (compact indices).
-__global__ void root_init_kernel(LinkBufs L, const int* total) {
-    const int n = *total;
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
-        const int p = L.pred[g];
-        L.root[g] = p < 0 ? g : p;
+// Trajectory roots (the first particle of each trajectory, compact index).
+// root[] is reset to -1, then every particle walks its pred chain until it
+// meets a particle whose root is already written or a trajectory start.
+// root[] only ever receives final values, so the walks need no barrier
+// between hops and the result is exact whatever the interleaving; particles
+// of early frames finish first and shorten the later walks.
+__device__ void roots_body(const LinkBufs& L, cg::grid_group& grid) {
+    const int n = L.off[L.T];
+    const int stride = gridDim.x * blockDim.x;
+    const int g0 = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int g = g0; g < n; g += stride) L.root[g] = -1;
+    grid.sync();
+    volatile int* root = L.root;
+    for (int g = g0; g < n; g += stride) {
+        int r = g;
+        while (true) {
+            const int known = root[r];
+            if (known >= 0) { r = known; break; }
+            const int p = __ldcg(L.pred + r);
+            if (p < 0) break;
+            r = p;
+        }
+        root[g] = r;
     }
 }
 
-__global__ void root_jump_kernel(LinkBufs L, const int* total) {
-    const int n = *total;
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x)
-        L.root[g] = L.root[L.root[g]];
+// The whole linker in one cooperative launch: link every frame with M = {},
+// then alternate {trajectory roots, memory entries M(t), relink frames whose
+// M changed} until no M changes (at most T + 1 passes).  ndirty[k] counts
+// the frames changed by pass k (zeroed by the host).
+namespace {
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+}  // namespace
+
+// phase_ns: [0] first linking, [1] roots, [2] memory entries, [3] relinking
+// (nanoseconds summed over passes, stamped by block 0 after each barrier)
+__global__ void __launch_bounds__(NTL, 4) link_fixpoint_kernel(LinkBufs L, int memory, int max_passes, int rounds,
+                                                               int* ndirty, int* passes,
+                                                               unsigned long long* phase_ns) {
+    cg::grid_group grid = cg::this_grid();
+    const bool stamp = blockIdx.x == 0 && threadIdx.x == 0;
+    unsigned long long t0 = stamp ? gtimer() : 0, acc[4] = {0, 0, 0, 0};
+    link_frames_body(L, 0);
+    int k = 0;
+    if (memory > 0 && L.T > 2) {
+        for (k = 1; k <= max_passes; ++k) {
+            grid.sync();
+            if (stamp) { const unsigned long long t = gtimer(); acc[k == 1 ? 0 : 3] += t - t0; t0 = t; }
+            roots_body(L, grid);
+            grid.sync();
+            if (stamp) { const unsigned long long t = gtimer(); acc[1] += t - t0; t0 = t; }
+            memory_body(L, memory, ndirty + k);
+            grid.sync();
+            if (stamp) { const unsigned long long t = gtimer(); acc[2] += t - t0; t0 = t; }
+            if (*(volatile int*)(ndirty + k) == 0) break;
+            link_frames_body(L, 1);
+        }
+    }
+    grid.sync();
+    if (stamp) { const unsigned long long t = gtimer(); acc[k <= 1 ? 0 : 3] += t - t0; t0 = t; }
+    roots_body(L, grid);
+    grid.sync();  // so that the last stamp covers every block's walk
+    if (stamp) {
+        acc[1] += gtimer() - t0;
+        *passes = k;
+        for (int i = 0; i < 4; ++i) phase_ns[i] = acc[i];
+    }
+    (void)rounds;
 }
 
 }  // namespace gt
