@@ -126,6 +126,24 @@ GT_API int gt_batch_device(gt_ctx* ctx, const void* d_frames, int dtype, int T, 
 GT_API int gt_link(gt_ctx* ctx, const float* rows, int64_t n, int ncols, float search_range,
             int has_memory, uint32_t memory, uint64_t* ids);
 
+/* Locate (no linking) ONE device-resident frame while allocating nothing:
+ * for callers that must not call cudaMalloc -- code running during CUDA
+ * stream capture, processes whose device memory belongs to another
+ * framework's pool, acquisition loops that forbid allocation once running.
+ * No counterpart in the reference.  Frames up to 2^20 pixels (H, W <= 8192)
+ * and 32768 features before the separation filter; sig_radius/bg_radius
+ * <= 31; search_range must be unset.  Writes min(*nrows, out_rows) rows of
+ * the gt_batch_device columns to d_out (device) and the row count to
+ * *nrows, on `stream` (a cudaStream_t, NULL = default stream), returning
+ * after the work has finished.  Scratch lives in one 16 MiB __device__ array
+ * per GPU, held until the process exits and shared by every call, which
+ * clears what must start at zero: calls that overlap on a GPU (other
+ * streams, other host threads) race and must be serialised by the caller.
+ * The first call on a device looks up that array's address; make it before
+ * any stream capture.  Errors: gt_last_error(NULL). */
+GT_API int gt_locate_frame_static(const void* d_frame, int dtype, int H, int W, const gt_params* params,
+                                  float* d_out, int64_t out_rows, int64_t* nrows, void* stream);
+
 /* Free a table returned by gt_batch. */
 GT_API void gt_table_free(gt_table* table);
 

@@ -96,6 +96,9 @@ SIGNATURES = [
     ("gt_table_free", None, [ctypes.POINTER(GtTable)]),
     ("gt_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GtStats)]),
     ("gt_ctx_set_option", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]),
+    ("gt_locate_frame_static", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.POINTER(GtParams), ctypes.c_void_p, ctypes.c_int64,
+                                              ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]),
 ]
 
 _lib = None

@@ -742,7 +742,12 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
 
 namespace {
 thread_local std::string g_noctx_err;  // errors of calls made without a context
+const char* g_noctx_override = nullptr;  // message of gt_locate_frame_static
 }
+
+namespace gt {
+void set_noctx_override(const char* msg) { g_noctx_override = msg; }
+}  // namespace gt
 
 extern "C" {
 
@@ -773,10 +778,14 @@ void gt_ctx_destroy(gt_ctx* ctx) {
     delete ctx;
 }
 
-const char* gt_last_error(const gt_ctx* ctx) { return ctx ? ctx->err.c_str() : g_noctx_err.c_str(); }
+const char* gt_last_error(const gt_ctx* ctx) {
+    if (ctx) return ctx->err.c_str();
+    return g_noctx_override ? g_noctx_override : g_noctx_err.c_str();
+}
 
 int gt_column_names(const gt_params* params, char* buf, size_t buflen) {
     if (!params || !buf) return -GT_ERR_ARG;
+    g_noctx_override = nullptr;
     Resolved r;
     int rc = resolve(params, &r, &g_noctx_err);
     if (rc) return -rc;
