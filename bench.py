@@ -255,8 +255,8 @@ def main():
         cands = stats[-1]["candidates"]
         rows = stats[-1]["particles"]
         # algorithmic bytes of one locate launch: frames read once (u16) +
-        # candidate records written (64 B each)
-        loc_bytes = T * H * W * 2 + cands * 64
+        # candidate records written (80 B each)
+        loc_bytes = T * H * W * 2 + cands * 80
         peak, kind = peaks()
         achieved = loc_bytes / (loc_ms / 1e3) / 1e9
         traffic = None

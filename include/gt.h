@@ -15,6 +15,11 @@
  *                      linking.rs:12-61 `FrameSubsetter`
  *   gt_column_names    execute_gpu.rs:197-226 `column_names`
  *
+ * Entry points with no reference counterpart (the adjoint of the locate
+ * path at fixed peaks; see the declarations below):
+ *   gt_batch_device_walk, gt_adjoint_forward, gt_adjoint_backward,
+ *   gt_adjoint_uncertainty
+ *
  * Conventions: plain pointers and sizes, no C++ or torch types.  Every call
  * returns a gt_status; on failure gt_last_error() describes it.  A context
  * is bound to one device, owns one CUDA stream and is not thread-safe.
@@ -121,6 +126,48 @@ GT_API int gt_batch_device(gt_ctx* ctx, const void* d_frames, int dtype, int T, 
                     const gt_params* params, float* d_out, int64_t out_rows,
                     int64_t* nrows, void* stream);
 
+/* gt_batch_device that also writes, for each output row r < out_rows, the
+ * walk record d_walk[5r .. 5r+4] = {frame, last-read row, last-read column,
+ * final row, final column} (int32, device).  The refined position is
+ * (final + centroid at the last-read pixel), so these records are the fixed
+ * peaks of the gt_adjoint_* calls.  No reference counterpart. */
+GT_API int gt_batch_device_walk(gt_ctx* ctx, const void* d_frames, int dtype, int T, int H, int W,
+                         const gt_params* params, float* d_out, int64_t out_rows,
+                         int64_t* nrows, int32_t* d_walk, void* stream);
+
+/* Bandpass + centroid refinement at fixed peaks (no reference counterpart;
+ * the forward arithmetic is that of centers.wgsl:23-109 and
+ * walk_cols.wgsl:38-74 over preprocess_rows/cols.wgsl).  d_frames: T x H x W
+ * f32 on the device; d_walk: n walk records (gt_batch_device_walk).
+ * Writes d_yxm (n x 3: y, x, mass), equal bit for bit to the located rows
+ * for the frames and parameters that produced the walk records.  Params
+ * follow gt_batch (diameter <= 31, max_iterations >= 1).  A walk record
+ * outside the frames returns GT_ERR_ARG. */
+GT_API int gt_adjoint_forward(gt_ctx* ctx, const float* d_frames, int T, int H, int W,
+                       const gt_params* params, const int32_t* d_walk, int64_t n,
+                       float* d_yxm, void* stream);
+
+/* Adjoint of gt_adjoint_forward: given dL/d(y, x, mass) (d_grad_yxm, n x 3),
+ * overwrites d_grad_frames (T x H x W f32, device) with dL/dframes and
+ * d_grad_params (2 doubles, device) with dL/dnoise_size and
+ * dL/dsmoothing_size.  The clip of the bandpass at 0 takes subgradient 0;
+ * smoothing_size is differentiated through the box normalisation 1/k^2
+ * treated as continuous in k (window and Gaussian taps held fixed).
+ * Gradients are summed with atomic additions: bitwise run-to-run equality
+ * is not guaranteed where particle circles overlap. */
+GT_API int gt_adjoint_backward(gt_ctx* ctx, const float* d_frames, int T, int H, int W,
+                        const gt_params* params, const int32_t* d_walk, int64_t n,
+                        const float* d_grad_yxm, float* d_grad_frames,
+                        double* d_grad_params, void* stream);
+
+/* Localisation uncertainty by linear propagation through the same Jacobian:
+ * pixel variance gain * max(I, 0) + read_noise^2 (Poisson counts scaled by
+ * the gain, plus read noise), independent pixels.  Writes the standard
+ * deviations of (y, x, mass) to d_sd (n x 3, device). */
+GT_API int gt_adjoint_uncertainty(gt_ctx* ctx, const float* d_frames, int T, int H, int W,
+                           const gt_params* params, const int32_t* d_walk, int64_t n,
+                           float gain, float read_noise, float* d_sd, void* stream);
+
 /* Link an (n x ncols) host f32 table whose columns 0, 2, 3 are frame, y, x
  * (link_rust's FrameSubsetter layout).  Writes n trajectory IDs. */
 GT_API int gt_link(gt_ctx* ctx, const float* rows, int64_t n, int ncols, float search_range,
@@ -170,6 +217,8 @@ typedef struct gt_stats {
     int32_t locate_kernel;     /* 0 generic, 1 specialised, 2 specialised with TMA staging */
     float link_phase_ms[4];    /* linker: first pass, roots, memory entries, relinking */
     int32_t link_dirty[8];     /* frames relinked by fixed-point passes 1..8 */
+    float ms_adjoint_particles; /* gt_adjoint_*: per-particle kernel */
+    float ms_adjoint_dense;     /* gt_adjoint_backward: zeroing + transposed bandpass */
 } gt_stats;
 
 GT_API int gt_last_stats(const gt_ctx* ctx, gt_stats* out);

@@ -254,6 +254,8 @@ float unrolled_sum(const float* xs, int n) {
 struct Feature {
     int origin;        // raster index of the originating pixel
     float y, x, mass;  // walk result (walk_cols.wgsl:69-73)
+    int ul, vl;        // pixel of the last centroid read (`idx`)
+    int up, vp;        // final position of the walk
     // cpu_processed (execute_gpu.rs:286-299, 346-352)
     float Rg, ecc, signal;
     // characterize=True (centers.wgsl:64-80 read at the originating pixel)
@@ -337,6 +339,8 @@ std::vector<Feature> locate_frame(const float* pic, int H, int W, const or_param
             Feature f{};
             f.origin = u0 * W + v0;
             f.y = (float)fy; f.x = (float)fx; f.mass = (float)fm;
+            f.ul = (int)(idx / W); f.vl = (int)(idx % W);
+            f.up = u; f.vp = v;
             if (p.cpu_processed) {
                 // execute_gpu.rs:165-172 gather at the originating pixel, then
                 // 286-299 and 346-352.  Emitted origins are interior, so the
@@ -597,7 +601,7 @@ std::vector<std::string> column_names(const or_params& p) {
 }
 
 int run_batch(const float* frames, int T, int H, int W, const or_params* pp, int nthreads,
-              int fp64, float** out, int64_t* nrows, int* ncols) {
+              int fp64, float** out, int64_t* nrows, int* ncols, int32_t** walk = nullptr) {
     const or_params p = *pp;
     if (p.has_bg_radius && !p.has_sig_radius) return 1;
     Circle cc = circle_table(p.diameter / 2);
@@ -647,6 +651,16 @@ int run_batch(const float* frames, int T, int H, int W, const or_params* pp, int
             if (p.has_bg_radius) { row[c++] = f.bg_median; row[c++] = f.corrected; }
             if (p.characterize) { row[c++] = f.g_rg; row[c++] = f.g_raw; row[c++] = f.g_sig; row[c++] = f.g_ecc; }
         }
+    if (walk) {
+        int32_t* wk = (int32_t*)std::malloc(sizeof(int32_t) * 5 * (size_t)std::max<int64_t>(nr, 1));
+        int64_t q = 0;
+        for (int t = 0; t < T; ++t)
+            for (const Feature& f : per[t]) {
+                int32_t* w5 = wk + 5 * q++;
+                w5[0] = t; w5[1] = f.ul; w5[2] = f.vl; w5[3] = f.up; w5[4] = f.vp;
+            }
+        *walk = wk;
+    }
     *out = o;
     *nrows = nr;
     *ncols = nc;
@@ -660,6 +674,11 @@ extern "C" {
 int or_batch(const float* frames, int T, int H, int W, const or_params* p, int nthreads,
              int fp64, float** out, int64_t* nrows, int* ncols) {
     return run_batch(frames, T, H, W, p, nthreads, fp64, out, nrows, ncols);
+}
+
+int or_batch_walk(const float* frames, int T, int H, int W, const or_params* p, int nthreads,
+                  float** out, int64_t* nrows, int* ncols, int32_t** walk) {
+    return run_batch(frames, T, H, W, p, nthreads, 0, out, nrows, ncols, walk);
 }
 
 int or_batch_u16(const uint16_t* frames, int T, int H, int W, const or_params* p, int nthreads,

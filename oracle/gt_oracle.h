@@ -55,6 +55,12 @@ typedef struct or_params {
 int or_batch(const float* frames, int T, int H, int W, const or_params* p,
              int nthreads, int fp64, float** out, int64_t* nrows, int* ncols);
 
+/* or_batch (FP32) that also returns, per output row, the walk record
+ * {frame, last-read row, last-read column, final row, final column}
+ * (malloc'd n x 5 int32; free with or_free). */
+int or_batch_walk(const float* frames, int T, int H, int W, const or_params* p, int nthreads,
+                  float** out, int64_t* nrows, int* ncols, int32_t** walk);
+
 /* Same as or_batch on uint16 pixels (converted exactly to f32). */
 int or_batch_u16(const uint16_t* frames, int T, int H, int W, const or_params* p,
                  int nthreads, int fp64, float** out, int64_t* nrows, int* ncols);

@@ -46,6 +46,9 @@ def load():
                                  ctypes.c_int, ctypes.c_int, ctypes.POINTER(fp), ctypes.POINTER(ctypes.c_int64),
                                  ctypes.POINTER(ctypes.c_int)]
         lib.or_batch_u16.argtypes = lib.or_batch.argtypes
+        lib.or_batch_walk.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(OrParams), ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p]
         lib.or_link.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                 ctypes.c_void_p]
         lib.or_bandpass.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
@@ -137,6 +140,31 @@ def batch(video, diameter, nthreads=1, fp64=False, **kw):
     if st != 0:
         raise RuntimeError(f"oracle status {st}")
     return tab, columns(p)
+
+
+def batch_walk(video, diameter, nthreads=1, **kw):
+    """FP32 batch on float32 frames plus the (n, 5) int32 walk records
+    {frame, last-read row, last-read column, final row, final column}."""
+    p = resolve(diameter, **kw)
+    arr = np.ascontiguousarray(video, dtype=np.float32)
+    T, H, W = arr.shape
+    lib = load()
+    out = ctypes.POINTER(ctypes.c_float)()
+    wk = ctypes.POINTER(ctypes.c_int32)()
+    nr = ctypes.c_int64()
+    nc = ctypes.c_int()
+    st = lib.or_batch_walk(arr.ctypes.data_as(ctypes.c_void_p), T, H, W, ctypes.byref(p), int(nthreads),
+                           ctypes.byref(out), ctypes.byref(nr), ctypes.byref(nc), ctypes.byref(wk))
+    try:
+        n, c = nr.value, nc.value
+        tab = np.ctypeslib.as_array(out, shape=(max(n, 1) * c,))[: n * c].copy().reshape(n, c)
+        walk = np.ctypeslib.as_array(wk, shape=(max(n, 1) * 5,))[: n * 5].copy().reshape(n, 5)
+    finally:
+        lib.or_free(out)
+        lib.or_free(wk)
+    if st != 0:
+        raise RuntimeError(f"oracle status {st}")
+    return tab, walk, columns(p)
 
 
 def link(table, search_range, memory=None):

@@ -76,6 +76,8 @@ class GtStats(ctypes.Structure):
         ("locate_kernel", ctypes.c_int32),
         ("link_phase_ms", ctypes.c_float * 4),
         ("link_dirty", ctypes.c_int32 * 8),
+        ("ms_adjoint_particles", ctypes.c_float),
+        ("ms_adjoint_dense", ctypes.c_float),
     ]
 
 
@@ -99,6 +101,20 @@ SIGNATURES = [
     ("gt_locate_frame_static", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                               ctypes.POINTER(GtParams), ctypes.c_void_p, ctypes.c_int64,
                                               ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]),
+    ("gt_batch_device_walk", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int, ctypes.POINTER(GtParams), ctypes.c_void_p,
+                                            ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p,
+                                            ctypes.c_void_p]),
+    ("gt_adjoint_forward", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.POINTER(GtParams), ctypes.c_void_p, ctypes.c_int64,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
+    ("gt_adjoint_backward", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.POINTER(GtParams), ctypes.c_void_p, ctypes.c_int64,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("gt_adjoint_uncertainty", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.POINTER(GtParams), ctypes.c_void_p,
+                                              ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_void_p,
+                                              ctypes.c_void_p]),
 ]
 
 _lib = None

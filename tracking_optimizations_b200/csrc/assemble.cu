@@ -70,6 +70,10 @@ __global__ void assemble_kernel(AsmArgs a) {
         row[c++] = x;
         if (a.has_link) row[c++] = (float)a.newid[a.root[g]];
         const Cand& rec = a.cand[(size_t)t * a.cap_c + a.prec[s]];
+        if (a.walk && g < a.walk_rows) {
+            int* wr = a.walk + (size_t)g * 5;
+            wr[0] = t; wr[1] = rec.ul; wr[2] = rec.vl; wr[3] = rec.up; wr[4] = rec.vp;
+        }
         if (a.cpu_processed) {
             // execute_gpu.rs:349-351
             row[c++] = sqrtf(rec.rg_sum / mass);

@@ -36,6 +36,10 @@ cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaSt
                                int* used_tma);
 cudaError_t launch_verify_division(float divisor, FixedDiv f, unsigned int* d_count, int num_sms,
                                    cudaStream_t st);
+cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* frames, const int* walk, long long n,
+                                     const int* circ, const float* grad, float* yxm, float* gR, double* gpar,
+                                     int* err, int num_sms, cudaStream_t st);
+cudaError_t launch_adjoint_transpose(const AdjParams& p, const float* gR, float* gI, cudaStream_t st);
 }  // namespace gt
 
 using namespace gt;
@@ -269,7 +273,7 @@ int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int 
     const int PH = LOC_TH + 2 * lp.hp, PW = LOC_TW + 2 * lp.hp;  // generic kernel plan
     const int RH = PH + 2 * lp.krad, RW = PW + 2 * lp.krad;
     P.smem_loc = sizeof(float) * ((size_t)RH * RW + 2 * (size_t)RH * PW + (size_t)PH * PW) +
-                 sizeof(int) * (size_t)LOC_TH * LOC_TW + 4 * sizeof(float) * LOC_CMAX + (size_t)LOC_TH * LOC_TW;
+                 sizeof(int) * (size_t)LOC_TH * LOC_TW + 6 * sizeof(float) * LOC_CMAX + (size_t)LOC_TH * LOC_TW;
     P.smem_loc = (P.smem_loc + 15) / 16 * 16;
     if (P.smem_loc > 227 * 1024) { *msg = "diameter/separation too large for the tile plan"; return GT_ERR_ARG; }
     P.fb_win = std::min(FB_WIN_MAX, std::max(lp.rint_c + 1, lp.max_iter - 1 + lp.rint_c + 1));
@@ -538,7 +542,7 @@ int fast_division(gt_ctx* ctx, const Plan& P, FixedDiv* dn, FixedDiv* dk, bool* 
 
 // The whole locate(+link) pipeline on device frames; table left in w.out.
 int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames, cudaStream_t st,
-                 int* err_bits, int64_t* nrows) {
+                 int* err_bits, int64_t* nrows, int* d_walk = nullptr, int64_t walk_rows = 0) {
     const int T = P.T;
     MovieBufs b = movie_bufs(P, w, d_frames);
     int rc = upload_tables(ctx, P, w, st);
@@ -609,6 +613,8 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
     a.sig_off = w.sig_off; a.n_sig = (int)P.sig_off.size() / 2;
     a.bg_off = w.bg_off; a.n_bg = (int)P.bg_off.size() / 2;
     a.out = w.out;
+    a.walk = d_walk;
+    a.walk_rows = walk_rows;
     assemble_kernel<<<T, 256, 0, st>>>(a);
     CK(cudaGetLastError());
     ctx->stats.launches += 1;
@@ -670,7 +676,7 @@ size_t elem_size(int dtype) { return dtype == GT_U16 ? 2 : 4; }
 
 int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, int H, int W,
                  const gt_params* params, gt_table* out_tab, float* d_out, int64_t out_rows,
-                 int64_t* nrows_out, cudaStream_t st) {
+                 int64_t* nrows_out, cudaStream_t st, int* d_walk = nullptr) {
     if (!ctx) return GT_ERR_ARG;
     ctx->err.clear();
     ctx->stats = gt_stats{};
@@ -678,7 +684,7 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
         ctx->err = "invalid frames/shape/dtype";
         return GT_ERR_ARG;
     }
-    if ((long long)H * W > (1LL << 28)) { ctx->err = "frame too large"; return GT_ERR_ARG; }
+    if ((long long)H * W > (1LL << 28) || H > 65535 || W > 65535) { ctx->err = "frame too large"; return GT_ERR_ARG; }
     Resolved r;
     int rc = resolve(params, &r, &ctx->err);
     if (rc) return rc;
@@ -701,7 +707,7 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
         }
         int bits = 0;
         int64_t nrows = 0;
-        rc = run_pipeline(ctx, P, w, dfr, st, &bits, &nrows);
+        rc = run_pipeline(ctx, P, w, dfr, st, &bits, &nrows, d_walk, d_walk ? out_rows : 0);
         if (rc) return rc;
         bool retry;
         rc = err_status(ctx, bits, &retry);
@@ -738,6 +744,114 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
     return GT_ERR_CAPACITY;
 }
 
+
+// Parameters of the gt_adjoint_* calls: the forward weights exactly as
+// make_plan derives them, the normalised taps a_i = w_i / sum(w) and
+// da_i / ds in double precision, and the centroid circle in the order of
+// the centroid loop (i outer, j inner, float mask <= r^2).
+int adjoint_setup(gt_ctx* ctx, const float* d_frames, int T, int H, int W, const gt_params* params,
+                  const int32_t* d_walk, int64_t n, AdjParams* ap, std::vector<int>* circ) {
+    if (!ctx) return GT_ERR_ARG;
+    ctx->err.clear();
+    ctx->stats = gt_stats{};
+    if (!d_frames || !params || T < 1 || H < 1 || W < 1 || n < 0 || (n > 0 && !d_walk)) {
+        ctx->err = "invalid frames/shape/walk";
+        return GT_ERR_ARG;
+    }
+    if ((long long)H * W > (1LL << 28) || H > 65535 || W > 65535) { ctx->err = "frame too large"; return GT_ERR_ARG; }
+    Resolved r;
+    int rc = resolve(params, &r, &ctx->err);
+    if (rc) return rc;
+    if (r.max_iterations < 1) {
+        ctx->err = "the adjoint needs max_iterations >= 1";
+        return GT_ERR_UNSUPPORTED;
+    }
+    if (r.diameter > 31) {
+        ctx->err = "the adjoint supports diameter <= 31";
+        return GT_ERR_UNSUPPORTED;
+    }
+    std::memset(ap, 0, sizeof(*ap));
+    ap->T = T; ap->H = H; ap->W = W;
+    const int k = (int)r.smoothing_size;
+    ap->krad = k / 2;
+    if (H <= ap->krad || W <= ap->krad) { ctx->err = "frame smaller than the smoothing window"; return GT_ERR_ARG; }
+    const float sigma2 = r.noise_size;
+    if (!(sigma2 > 0.0f)) { ctx->err = "noise_size must be > 0"; return GT_ERR_ARG; }
+    float norm = 0.0f;
+    double sw = 0.0, swi = 0.0;
+    for (int i = -ap->krad; i <= ap->krad; ++i) {
+        const float x = (float)i;
+        const float g = std::exp(-x * x / (2.0f * sigma2));
+        ap->w[i + ap->krad] = g;
+        norm = norm + g;
+        const double gd = std::exp(-(double)i * i / (2.0 * sigma2));
+        sw += gd;
+        swi += gd * i * i;
+    }
+    ap->norm = norm;
+    ap->kk = (float)(k * k);
+    const double s2 = (double)sigma2 * sigma2;
+    for (int i = -ap->krad; i <= ap->krad; ++i) {
+        const double ai = std::exp(-(double)i * i / (2.0 * sigma2)) / sw;
+        ap->a[i + ap->krad] = (float)ai;
+        // d/ds [exp(-i^2 / 2s) / sum_j exp(-j^2 / 2s)] = a_i (i^2 - <j^2>) / (2 s^2)
+        ap->da[i + ap->krad] = (float)(ai * ((double)i * i - swi / sw) / (2.0 * s2));
+    }
+    ap->k = (float)k;
+    ap->rc = ((int)r.diameter - 1) / 2;
+    ap->border = (int)r.diameter / 2;
+    circ->clear();
+    const float rr = (float)ap->rc;
+    const float r2 = rr * rr;
+    for (int i = -ap->rc; i <= ap->rc; ++i)
+        for (int j = -ap->rc; j <= ap->rc; ++j) {
+            const float x = (float)i, y = (float)j;
+            if (x * x + y * y > r2) continue;
+            circ->push_back(i);
+            circ->push_back(j);
+        }
+    ap->K = (int)circ->size() / 2;
+    ap->gain = 1.0f;
+    ap->read_var = 0.0f;
+    CK(cudaSetDevice(ctx->device));
+    return GT_OK;
+}
+
+// Scratch of the gt_adjoint_* calls in the context arena: the error word,
+// the circle table and (backward only) the dL/dR plane.
+struct AdjWork {
+    int* err;
+    int* circ;
+    float* plane;
+};
+
+int adjoint_work(gt_ctx* ctx, const AdjParams& ap, const std::vector<int>& circ, bool plane, AdjWork* aw,
+                 cudaStream_t st) {
+    const size_t off_circ = 256;
+    const size_t off_plane = off_circ + ((sizeof(int) * circ.size() + 255) / 256) * 256;
+    const size_t need = off_plane + (plane ? sizeof(float) * (size_t)ap.T * ap.H * ap.W : 0);
+    int rc = ensure_arena(ctx, need);
+    if (rc) return rc;
+    aw->err = (int*)ctx->arena;
+    aw->circ = (int*)(ctx->arena + off_circ);
+    aw->plane = plane ? (float*)(ctx->arena + off_plane) : nullptr;
+    CK(cudaMemsetAsync(aw->err, 0, sizeof(int), st));
+    CK(cudaMemcpyAsync(aw->circ, circ.data(), sizeof(int) * circ.size(), cudaMemcpyHostToDevice, st));
+    for (int i = 0; i < 3; ++i)
+        if (!ctx->ev[i]) CK(cudaEventCreate(&ctx->ev[i]));
+    return GT_OK;
+}
+
+int adjoint_finish(gt_ctx* ctx, const AdjWork& aw, cudaStream_t st) {
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, aw.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr) {
+        ctx->err = "a walk record lies outside the frames";
+        return GT_ERR_ARG;
+    }
+    return GT_OK;
+}
 }  // namespace
 
 namespace {
@@ -815,6 +929,103 @@ int gt_batch_device(gt_ctx* ctx, const void* d_frames, int dtype, int T, int H, 
                     const gt_params* params, float* d_out, int64_t out_rows, int64_t* nrows, void* stream) {
     cudaStream_t st = stream ? (cudaStream_t)stream : (ctx ? ctx->stream : nullptr);
     return batch_common(ctx, d_frames, false, dtype, T, H, W, params, nullptr, d_out, out_rows, nrows, st);
+}
+
+int gt_batch_device_walk(gt_ctx* ctx, const void* d_frames, int dtype, int T, int H, int W,
+                         const gt_params* params, float* d_out, int64_t out_rows, int64_t* nrows, int32_t* d_walk,
+                         void* stream) {
+    if (ctx && !d_walk && out_rows > 0) {
+        ctx->err = "null walk buffer";
+        return GT_ERR_ARG;
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : (ctx ? ctx->stream : nullptr);
+    return batch_common(ctx, d_frames, false, dtype, T, H, W, params, nullptr, d_out, out_rows, nrows, st,
+                        (int*)d_walk);
+}
+
+int gt_adjoint_forward(gt_ctx* ctx, const float* d_frames, int T, int H, int W, const gt_params* params,
+                       const int32_t* d_walk, int64_t n, float* d_yxm, void* stream) {
+    AdjParams ap;
+    std::vector<int> circ;
+    int rc = adjoint_setup(ctx, d_frames, T, H, W, params, d_walk, n, &ap, &circ);
+    if (rc) return rc;
+    if (n > 0 && !d_yxm) { ctx->err = "null output"; return GT_ERR_ARG; }
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    AdjWork aw;
+    rc = adjoint_work(ctx, ap, circ, false, &aw, st);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[0], st));
+    CK(launch_adjoint_particles(0, ap, d_frames, d_walk, n, aw.circ, nullptr, d_yxm, nullptr, nullptr, aw.err,
+                                ctx->num_sms, st));
+    CK(cudaEventRecord(ctx->ev[1], st));
+    ctx->stats.launches = n > 0 ? 1 : 0;
+    rc = adjoint_finish(ctx, aw, st);
+    cudaEventElapsedTime(&ctx->stats.ms_adjoint_particles, ctx->ev[0], ctx->ev[1]);
+    ctx->stats.ms_total = ctx->stats.ms_adjoint_particles;
+    return rc;
+}
+
+int gt_adjoint_backward(gt_ctx* ctx, const float* d_frames, int T, int H, int W, const gt_params* params,
+                        const int32_t* d_walk, int64_t n, const float* d_grad_yxm, float* d_grad_frames,
+                        double* d_grad_params, void* stream) {
+    AdjParams ap;
+    std::vector<int> circ;
+    int rc = adjoint_setup(ctx, d_frames, T, H, W, params, d_walk, n, &ap, &circ);
+    if (rc) return rc;
+    if (!d_grad_frames || !d_grad_params || (n > 0 && !d_grad_yxm)) { ctx->err = "null output"; return GT_ERR_ARG; }
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    AdjWork aw;
+    rc = adjoint_work(ctx, ap, circ, true, &aw, st);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(d_grad_params, 0, 2 * sizeof(double), st));
+    CK(cudaEventRecord(ctx->ev[0], st));
+    CK(cudaMemsetAsync(aw.plane, 0, sizeof(float) * (size_t)T * H * W, st));
+    CK(cudaEventRecord(ctx->ev[1], st));
+    CK(launch_adjoint_particles(1, ap, d_frames, d_walk, n, aw.circ, d_grad_yxm, nullptr, aw.plane, d_grad_params,
+                                aw.err, ctx->num_sms, st));
+    CK(cudaEventRecord(ctx->ev[2], st));
+    CK(launch_adjoint_transpose(ap, aw.plane, d_grad_frames, st));
+    ctx->stats.launches = (n > 0 ? 1 : 0) + (T + 65534) / 65535;
+    // the dense part is the zeroing plus the transposed bandpass
+    if (!ctx->ev[3]) CK(cudaEventCreate(&ctx->ev[3]));
+    CK(cudaEventRecord(ctx->ev[3], st));
+    rc = adjoint_finish(ctx, aw, st);
+    cudaEventElapsedTime(&ctx->stats.ms_adjoint_particles, ctx->ev[1], ctx->ev[2]);
+    float tz = 0.f, tt = 0.f;
+    cudaEventElapsedTime(&tz, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&tt, ctx->ev[2], ctx->ev[3]);
+    ctx->stats.ms_adjoint_dense = tz + tt;
+    cudaEventElapsedTime(&ctx->stats.ms_total, ctx->ev[0], ctx->ev[3]);
+    return rc;
+}
+
+int gt_adjoint_uncertainty(gt_ctx* ctx, const float* d_frames, int T, int H, int W, const gt_params* params,
+                           const int32_t* d_walk, int64_t n, float gain, float read_noise, float* d_sd,
+                           void* stream) {
+    AdjParams ap;
+    std::vector<int> circ;
+    int rc = adjoint_setup(ctx, d_frames, T, H, W, params, d_walk, n, &ap, &circ);
+    if (rc) return rc;
+    if (n > 0 && !d_sd) { ctx->err = "null output"; return GT_ERR_ARG; }
+    if (!(gain >= 0.0f) || !(read_noise >= 0.0f) || !std::isfinite(gain) || !std::isfinite(read_noise)) {
+        ctx->err = "gain and read_noise must be finite and >= 0";
+        return GT_ERR_ARG;
+    }
+    ap.gain = gain;
+    ap.read_var = read_noise * read_noise;
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    AdjWork aw;
+    rc = adjoint_work(ctx, ap, circ, false, &aw, st);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[0], st));
+    CK(launch_adjoint_particles(2, ap, d_frames, d_walk, n, aw.circ, nullptr, d_sd, nullptr, nullptr, aw.err,
+                                ctx->num_sms, st));
+    CK(cudaEventRecord(ctx->ev[1], st));
+    ctx->stats.launches = n > 0 ? 1 : 0;
+    rc = adjoint_finish(ctx, aw, st);
+    cudaEventElapsedTime(&ctx->stats.ms_adjoint_particles, ctx->ev[0], ctx->ev[1]);
+    ctx->stats.ms_total = ctx->stats.ms_adjoint_particles;
+    return rc;
 }
 
 int gt_ctx_set_option(gt_ctx* ctx, const char* key, int value) {

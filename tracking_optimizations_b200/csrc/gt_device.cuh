@@ -65,7 +65,9 @@ __device__ __forceinline__ bool centroid_at(const LocParams& p, const Acc& P, in
 
 struct WalkOut {
     float y, x, mass;
-    int ok;  // 0 when the accessor could not serve a step
+    int ok;      // 0 when the accessor could not serve a step
+    int ul, vl;  // pixel of the last centroid read
+    int up, vp;  // final position
 };
 
 // walk_cols.wgsl:38-74.  WGSL zero-initialises `center` and `idx`; with
@@ -75,8 +77,10 @@ __device__ __forceinline__ WalkOut walk_from(const LocParams& p, const Acc& P, i
     WalkOut o;
     float c0 = 0.f, c1 = 0.f, m = 0.f;
     const float thr = p.thr;
+    o.ul = 0; o.vl = 0;  // WGSL zero-initialised idx
     for (int it = 0; it < p.max_iter; ++it) {
         if (!centroid_at(p, P, u, v, c0, c1, m)) { o.ok = 0; o.y = o.x = o.mass = 0.f; return o; }
+        o.ul = u; o.vl = v;
         bool changed = false;
         if (c0 > thr && u < p.H - 1) { u += 1; changed = true; }
         else if (c0 < -thr && u > 0) { u -= 1; changed = true; }
@@ -88,6 +92,7 @@ __device__ __forceinline__ WalkOut walk_from(const LocParams& p, const Acc& P, i
     o.x = (float)v + c1;
     o.mass = m;
     o.ok = 1;
+    o.up = u; o.vp = v;
     return o;
 }
 

@@ -50,7 +50,9 @@ struct __align__(16) Cand {
     float mid;            // processed value at the originating pixel
     float signal;
     float g_rg, g_raw, g_sig, g_ecc;   // characterize=True columns
-    float pad;
+    int ul, vl;           // pixel of the walk's last centroid read
+    int up, vp;           // walk's final position (differs when the walk ran out)
+    int pad;
 };
 
 enum CandState { CAND_EMIT = 0, CAND_PENDING = 1, CAND_REJECT = 2 };
@@ -151,6 +153,24 @@ struct LinkBufs {
     int lsm_bytes;        // dynamic shared memory pool of the linker blocks
 };
 
+// Adjoint of bandpass + refine at fixed peaks.  The forward arithmetic uses
+// the same weights as LocParams; a / da are the real-valued normalised
+// Gaussian taps w_i / sum(w) and their derivative with respect to
+// noise_size (the Gaussian variance).
+struct AdjParams {
+    int T, H, W;
+    int krad;                // smoothing half window
+    int rc;                  // centroid circle radius, (diameter - 1) / 2
+    int border;              // diameter / 2: centroids inside this band are zero
+    int K;                   // circle pixel count
+    float w[GT_MAX_TAPS];    // forward weights, as LocParams::w
+    float norm, kk;          // forward normaliser and f32(k * k)
+    float a[GT_MAX_TAPS];    // w_i / sum(w)
+    float da[GT_MAX_TAPS];   // d a_i / d noise_size
+    float k;                 // smoothing_size as a real number
+    float gain, read_var;    // noise model of the uncertainty kernel
+};
+
 struct AsmArgs {
     int T, H, W, cap_p, cap_c, ncols;
     int has_link, cpu_processed, characterize, sig, bg;
@@ -170,6 +190,8 @@ struct AsmArgs {
     const int* bg_off;    // n_bg x {di, dj}, annulus_inds
     int n_bg;
     float* out;
+    int* walk;            // optional n x 5 {frame, last-read row, col, final row, col}
+    long long walk_rows;  // rows of `walk` (rows beyond are not written)
 };
 
 }  // namespace gt

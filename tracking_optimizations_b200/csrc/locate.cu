@@ -71,7 +71,9 @@ __global__ void __launch_bounds__(NT) locate_tiles_kernel(const LocParams p, con
     float* wx = wy + CMAX;
     float* wm = wx + CMAX;
     int* wst = (int*)(wm + CMAX);
-    unsigned char* flags = (unsigned char*)(wst + CMAX);
+    unsigned int* wlp = (unsigned int*)(wst + CMAX);  // last-read pixel (u << 16 | v)
+    unsigned int* wfp = wlp + CMAX;                   // final position (u << 16 | v)
+    unsigned char* flags = (unsigned char*)(wfp + CMAX);
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const size_t fbase = (size_t)t * H * W;
@@ -191,6 +193,7 @@ __global__ void __launch_bounds__(NT) locate_tiles_kernel(const LocParams p, con
             const int u0 = ty0 + q / TW, v0 = tx0 + q % TW;
             int st;
             float y = 0.f, x = 0.f, m = 0.f;
+            unsigned int lp = 0, fp = 0;
             if (p.max_iter <= 0) {
                 st = CAND_PENDING;  // mass read at pixel 0: resolved by the fallback kernel
             } else {
@@ -200,9 +203,11 @@ __global__ void __launch_bounds__(NT) locate_tiles_kernel(const LocParams p, con
                 } else {
                     y = wo.y; x = wo.x; m = wo.mass;
                     st = (m > p.minmass && m != 0.f) ? CAND_EMIT : CAND_REJECT;
+                    lp = ((unsigned)wo.ul << 16) | (unsigned)wo.vl;
+                    fp = ((unsigned)wo.up << 16) | (unsigned)wo.vp;
                 }
             }
-            wy[c] = y; wx[c] = x; wm[c] = m; wst[c] = st;
+            wy[c] = y; wx[c] = x; wm[c] = m; wst[c] = st; wlp[c] = lp; wfp[c] = fp;
         }
         __syncthreads();
         const int cchunk = (nr + NT - 1) / NT;
@@ -241,7 +246,9 @@ __global__ void __launch_bounds__(NT) locate_tiles_kernel(const LocParams p, con
             rec.state = wst[c];
             rec.rg_sum = rec.eccn = rec.mid = rec.signal = 0.f;
             rec.g_rg = rec.g_raw = rec.g_sig = rec.g_ecc = 0.f;
-            rec.pad = 0.f;
+            rec.ul = (int)(wlp[c] >> 16); rec.vl = (int)(wlp[c] & 0xffffu);
+            rec.up = (int)(wfp[c] >> 16); rec.vp = (int)(wfp[c] & 0xffffu);
+            rec.pad = 0;
             if (p.cpu_processed) cpu_features(p, b, acc, u0, v0, rec);
             if (p.characterize) gpu_features(p, b, acc, racc, u0, v0, rec);
             if (base >= 0) {
@@ -326,6 +333,7 @@ __global__ void __launch_bounds__(128) fallback_walk_kernel(const LocParams p, c
             WinAcc acc{wsm, y0, x0, n};
             float y, x, m;
             bool ok = true;
+            int ul = 0, vl = 0, up = u0, vp = v0;
             if (p.max_iter <= 0) {
                 // walk_cols.wgsl:69-73 with no iteration: offset (0, 0) and the
                 // mass of pixel 0, which is interior only when d/2 == 0 (its
@@ -336,12 +344,14 @@ __global__ void __launch_bounds__(128) fallback_walk_kernel(const LocParams p, c
                 WalkOut wo = walk_from(p, acc, u0, v0);
                 ok = wo.ok != 0;
                 y = wo.y; x = wo.x; m = wo.mass;
+                ul = wo.ul; vl = wo.vl; up = wo.up; vp = wo.vp;
             }
             if (!ok) {  // window too small for this walk: report, never guess
                 atomicOr(b.err, ERR_SCRATCH_OVERFLOW);
                 rec->state = CAND_REJECT;
             } else {
                 rec->y = y; rec->x = x; rec->mass = m;
+                rec->ul = ul; rec->vl = vl; rec->up = up; rec->vp = vp;
                 rec->state = (m > p.minmass && m != 0.f) ? CAND_EMIT : CAND_REJECT;
             }
         }

@@ -74,7 +74,7 @@ struct Geo {
     static constexpr int RPA = 4 * NRQ + KR;  // Gp/Bp row pairs allocated
     static constexpr int SZ_RP = align128(cmax(RP * RPS * 8, 4 * NRQ * P2S * 8));
     static constexpr int SZ_GP = align128(cmax(cmax(RPA * GPS * 8, (PP + 1) * RMS * 8), TH0 * FT * 4));
-    static constexpr int SZ_BP = align128(cmax(cmax(RPA * GPS * 8, RH * RW * 2), TH0 * FT + 4 * 4 * FCMAX));
+    static constexpr int SZ_BP = align128(cmax(cmax(RPA * GPS * 8, RH * RW * 2), TH0 * FT + 6 * 4 * FCMAX));
     static constexpr int K = circle_size(RC);
     static constexpr int SZ_TAB = align128(K * 8);
     static constexpr int OFF_GP = SZ_RP;
@@ -306,6 +306,8 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     float* wx = wy + FCMAX;
     float* wm = wx + FCMAX;
     int* wst = (int*)(wm + FCMAX);
+    unsigned int* wlp = (unsigned int*)(wst + FCMAX);  // last-read pixel (u << 16 | v)
+    unsigned int* wfp = wlp + FCMAX;                   // final position (u << 16 | v)
     float2* sc = (float2*)(smem + G::OFF_TAB);  // (sin2, cos2) of the d/2 circle
 
     // ---- 0. stage the raw tile ----
@@ -550,6 +552,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
             const int u0 = ty0 + q / FT, v0 = tx0 + q % FT;
             int st;
             float y = 0.f, x = 0.f, m = 0.f;
+            unsigned int lp = 0, fp = 0;
             if (p.max_iter <= 0) {
                 st = CAND_PENDING;
             } else {
@@ -559,6 +562,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
                 bool ok = true;
                 for (int iter = 0; iter < p.max_iter; ++iter) {
                     if (!centroid_fixed<G, RC>(p, acc, u, v, c0, c1, m)) { ok = false; break; }
+                    lp = ((unsigned)u << 16) | (unsigned)v;
                     bool changed = false;
                     if (c0 > p.thr && u < H - 1) { u += 1; changed = true; }
                     else if (c0 < -p.thr && u > 0) { u -= 1; changed = true; }
@@ -573,9 +577,10 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
                     y = (float)u + c0;
                     x = (float)v + c1;
                     st = (m > p.minmass && m != 0.f) ? CAND_EMIT : CAND_REJECT;
+                    fp = ((unsigned)u << 16) | (unsigned)v;
                 }
             }
-            wy[c] = y; wx[c] = x; wm[c] = m; wst[c] = st;
+            wy[c] = y; wx[c] = x; wm[c] = m; wst[c] = st; wlp[c] = lp; wfp[c] = fp;
         }
         __syncthreads();
         const int cchunk = (nr + FNT - 1) / FNT;
@@ -614,7 +619,9 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
             rec.state = wst[c];
             rec.rg_sum = rec.eccn = rec.mid = rec.signal = 0.f;
             rec.g_rg = rec.g_raw = rec.g_sig = rec.g_ecc = 0.f;
-            rec.pad = 0.f;
+            rec.ul = (int)(wlp[c] >> 16); rec.vl = (int)(wlp[c] & 0xffffu);
+            rec.up = (int)(wfp[c] >> 16); rec.vp = (int)(wfp[c] & 0xffffu);
+            rec.pad = 0;
             if (p.cpu_processed) {
                 // execute_gpu.rs:165-172, 286-299 at the originating pixel
                 const int rr = u0 - py0, cc = v0 - px0;

@@ -333,7 +333,7 @@ extern "C" int gt_locate_frame_static(const void* d_frame, int dtype, int H, int
         const int PH = 32 + 2 * lp.hp, PW = 64 + 2 * lp.hp;
         const int RH = PH + 2 * lp.krad, RW = PW + 2 * lp.krad;
         size_t smem = sizeof(float) * ((size_t)RH * RW + 2 * (size_t)RH * PW + (size_t)PH * PW) +
-                      sizeof(int) * 32 * 64 + 4 * sizeof(float) * 512 + 32 * 64;
+                      sizeof(int) * 32 * 64 + 6 * sizeof(float) * 512 + 32 * 64;
         smem = (smem + 15) / 16 * 16;
         if (smem > 227 * 1024) return fail(GT_ERR_ARG, "diameter/separation too large for the tile plan");
         SCK(cudaFuncSetAttribute(locate_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
