@@ -17,9 +17,7 @@ import argparse
 import ctypes
 import json
 import os
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -28,6 +26,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "locate+link frames/s at 512²×1000 u16"
+LOCATE_KERNELS = {0: "locate_tiles_kernel", 1: "locate_fast_kernel", 2: "locate_fast_kernel (TMA staging)"}
 
 
 def workload():
@@ -56,59 +55,99 @@ def peaks():
         return 6650.0, "fallback"
 
 
-class Clocks:
-    """nvidia-smi samples during the timed region."""
+def locate_traffic(frames):
+    """DRAM bytes (read + write) of one locate launch over `frames` frames:
+    the per-frame figure of the committed ncu capture of the same kernel on
+    300 frames of this workload (profiles/locate_fast_kernel_300x512.md),
+    scaled by the frame count (traffic is per frame)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "locate_fast_kernel_300x512.md")) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_frame:"):
+                    return int(line.split(":")[1]) * frames
+    except OSError:
+        pass
+    return None
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.path = None
+
+class Clocks:
+    """SM clock and clock-event reasons sampled through NVML (read-only) by a
+    background thread every ~2 ms, kept for the samples taken inside the
+    timed region (between __enter__ and __exit__)."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
+
+    def __init__(self, cuda_index):
+        self.cuda_index = cuda_index
+        self.samples = []
+        self.handle = None
+        self.thread = None
+        self.stop = None
+        self.t0 = self.t1 = None
+
+    def _open(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        self.nvml = pynvml
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            self.handle = pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+        except Exception:
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
+        self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+        self.reasons_fn = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                mhz = self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM)
+                rs = self.reasons_fn(self.handle)
+                self.samples.append((time.perf_counter(), mhz, rs))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        import threading
+
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            self._open()
         except Exception:
-            self.proc = None
+            self.handle = None
+            return self
+        self.stop = threading.Event()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+        deadline = time.perf_counter() + 2.0
+        while not self.samples and time.perf_counter() < deadline:
+            time.sleep(0.001)
+        self.t0 = time.perf_counter()
         return self
 
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
-
-    def summary(self):
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        self.t1 = time.perf_counter()
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=2)
         try:
-            for line in open(self.path):
-                f = [x.strip() for x in line.split(",")]
-                if len(f) < 9:
-                    continue
-                try:
-                    sm.append(float(f[1]))
-                    mx.append(float(f[2]))
-                except ValueError:
-                    continue
-                for n, v in zip(names, f[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(n)
-            os.unlink(self.path)
+            if self.handle is not None:
+                self.nvml.nvmlShutdown()
         except Exception:
             pass
-        if not sm:
+
+    def summary(self):
+        if self.handle is None or self.t0 is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        inside = [x for x in self.samples if self.t0 <= x[0] <= self.t1]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        reasons = sorted({n for _, _, rs in inside for n, bit in self.REASONS if rs & bit})
+        return {"sm_mhz": float(np.median([m for _, m, _ in inside])), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(inside), "source": "NVML every ~2 ms in the timed region"}
 
 
 def cpu_baseline(movie, params, budget_s=12.0):
@@ -160,6 +199,113 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args, rank, world, local):
+    """--workload adjoint: one step = the fixed-peak forward plus its adjoint
+    (gt_adjoint_forward + gt_adjoint_backward) over 256 frames of 512 x 512
+    f32 with the locate workload's spot model; peaks from one locate before
+    timing.  Algorithmic bytes per frame: the frame re-read (H*W*4) plus the
+    gradient write (H*W*4)."""
+    import torch
+
+    from tracking_optimizations_b200 import _native, adjoint, synth
+
+    torch.cuda.set_device(local)
+    spec, params = workload()
+    rspec = synth.scaled(spec, frames=args.frames or 256, seed=spec.seed + 100 + rank)
+    movie = synth.make_movie(rspec).astype(np.float32)
+    T, H, W = movie.shape
+    dev = f"cuda:{local}"
+    frames = torch.from_numpy(movie).to(dev)
+    aparams = {k: v for k, v in params.items() if k not in ("search_range", "memory", "cpu_processed")}
+    d = aparams.pop("diameter")
+    rows, walk, _ = adjoint.locate_with_walk(frames, d, **aparams)
+    n = walk.shape[0]
+    lib = _native.load()
+    ctx = _native.context(local)
+    gp = _native.make_params(d, **aparams)
+    yxm = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    gup = torch.randn((n, 3), device=dev, generator=torch.Generator(device=dev).manual_seed(0))
+    gI = torch.empty_like(frames)
+    gpar = torch.empty(2, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    st_f, st_b = [], []
+
+    def step():
+        _native.check(lib.gt_adjoint_forward(ctx, P(frames), T, H, W, ctypes.byref(gp), P(walk), n, P(yxm), sp),
+                      ctx)
+        st_f.append(_native.last_stats(local))
+        _native.check(lib.gt_adjoint_backward(ctx, P(frames), T, H, W, ctypes.byref(gp), P(walk), n, P(gup),
+                                              P(gI), P(gpar), sp), ctx)
+        st_b.append(_native.last_stats(local))
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    assert torch.equal(yxm, rows[:, [2, 3, 1]]), "fixed-peak forward differs from the located rows"
+    st_f.clear()
+    st_b.clear()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    # end to end: pinned host frames in, host gradient out, through the
+    # autograd Function
+    pinned = torch.from_numpy(movie).pin_memory()
+    host_grad = torch.empty((T, H, W), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        fr = pinned.to(dev, non_blocking=True).requires_grad_(True)
+        out = adjoint.refine(fr, walk, d, **aparams)
+        out.backward(gup)
+        host_grad.copy_(fr.grad, non_blocking=True)
+        torch.cuda.synchronize()
+
+    e2e_step()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if rank != 0:
+        return
+    med = lambda xs, k: float(np.median([x[k] for x in xs]))  # noqa: E731
+    dense_ms = med(st_b, "ms_adjoint_dense")
+    alg = T * H * W * 8
+    peak, kind = peaks()
+    achieved = alg / (ms / 1e3) / 1e9
+    line = {
+        "metric": "adjoint frames/s (fixed-peak forward + backward, 256 x 512x512 f32)",
+        "value": T / (ms / 1e3), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"adjoint at fixed peaks, {T} frames x {H}x{W} float32, {n} particles, "
+                               "locate spot model; gt_adjoint_forward + gt_adjoint_backward per step",
+                   "frames": T, "height": H, "width": W, "particles": n, "params": dict(aparams, diameter=d),
+                   "l2": f"inputs larger than L2 ({movie.nbytes >> 20} MB frames + gradient per step)"},
+        "roofline": {"bound": "hbm", "kernel": "whole step (frame re-read + gradient write)",
+                     "achieved": achieved, "peak": peak, "peak_kind": kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes": alg},
+        "stages_ms": {"forward_particles": med(st_f, "ms_adjoint_particles"),
+                      "backward_particles": med(st_b, "ms_adjoint_particles"),
+                      "backward_dense": dense_ms,
+                      "dense_achieved_gbs": T * H * W * 12 / (dense_ms / 1e3) / 1e9},
+        "gpu_launches": int(sum(x["launches"] for x in st_f + st_b)) // max(1, len(st_f)) * args.steps,
+        "e2e": {"value": T / (e2e_ms / 1e3), "unit": "frames/s", "h2d_bytes_per_step": int(movie.nbytes),
+                "d2h_bytes_per_step": int(movie.nbytes), "timing": "CUDA events around H2D + autograd + D2H"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -168,6 +314,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="locate-link", choices=["locate-link", "adjoint"])
     ap.add_argument("--frames", type=int, default=None,
                     help="smaller movie of the same spot model (profiling captures only)")
     args = ap.parse_args()
@@ -176,6 +323,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args, rank, world, local)
         return
 
     import torch
@@ -259,19 +409,14 @@ def main():
         loc_bytes = T * H * W * 2 + cands * 80
         peak, kind = peaks()
         achieved = loc_bytes / (loc_ms / 1e3) / 1e9
-        traffic = None
-        try:
-            with open(os.path.join(ROOT, "profiles", "locate_traffic.json")) as f:
-                tr = json.load(f)
-            traffic = tr["dram_bytes_per_frame"] * T
-        except Exception:
-            pass
+        traffic = locate_traffic(T)
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u16 in / f32 compute", "data": "synthetic",
             "config": config_dict(spec, params, world),
-            "roofline": {"bound": "hbm", "kernel": "locate_tiles_kernel", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": LOCATE_KERNELS.get(stats[-1]["locate_kernel"], "?"),
+                         "achieved": achieved, "peak": peak,
                          "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes": loc_bytes, "launch_ms": loc_ms},
             "stages_ms": {k: float(np.median([s[k] for s in stats]))
