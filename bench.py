@@ -306,6 +306,109 @@ def run_adjoint(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, rank, world, local):
+    """--workload batched: 64 uneven movies (synth.batch_workload, rendered
+    on the device), located and linked by one gt_batch_many_device call per
+    step (a replayed CUDA graph), against the plain path: one
+    gt_batch_device call per movie.  value = aggregate frames/s of the
+    batched call; the plain path's figure and the ratio are reported
+    beside it."""
+    import torch
+
+    from tracking_optimizations_b200 import _native, batched, synth
+
+    torch.cuda.set_device(local)
+    specs = synth.batch_workload()
+    if args.frames:
+        specs = specs[: args.frames]
+    t0 = time.perf_counter()
+    movies = [(synth.make_movie_device(s, f"cuda:{local}"), dict(s.params)) for s in specs]
+    gen_s = time.perf_counter() - t0
+    outs = batched.output_buffers(movies)
+    lib = _native.load()
+    ctx = _native.context(local)
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    arr = (_native.GtMovie * len(movies))()
+    plain_params = []
+    for i, ((fr, params), out) in enumerate(zip(movies, outs)):
+        kw = dict(params)
+        d = kw.pop("diameter")
+        m = arr[i]
+        m.frames = fr.data_ptr()
+        m.dtype = _native.GT_U16
+        m.T, m.H, m.W = fr.shape
+        m.params = _native.make_params(d, **kw)
+        m.out = out.data_ptr()
+        m.out_rows = out.shape[0]
+        plain_params.append(m.params)
+    nrows = ctypes.c_int64()
+    plain_rows = [0] * len(movies)
+
+    def plain_step():
+        for i, ((fr, _), out) in enumerate(zip(movies, outs)):
+            T, H, W = fr.shape
+            _native.check(lib.gt_batch_device(ctx, ctypes.c_void_p(fr.data_ptr()), _native.GT_U16, T, H, W,
+                                              ctypes.byref(plain_params[i]), ctypes.c_void_p(out.data_ptr()),
+                                              out.shape[0], ctypes.byref(nrows), sp), ctx)
+            plain_rows[i] = nrows.value
+
+    stats = []
+
+    def batch_step():
+        _native.check(lib.gt_batch_many_device(ctx, arr, len(movies), sp), ctx)
+        stats.append(_native.last_stats(local))
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    for _ in range(max(3, args.warmup)):
+        plain_step()
+    plain_ms = timed(plain_step, args.steps)
+    for _ in range(max(3, args.warmup)):
+        batch_step()
+    assert [arr[i].nrows for i in range(len(movies))] == plain_rows, "batched row counts differ from plain"
+    stats.clear()
+    with Clocks(local) as clk:
+        batch_ms = timed(batch_step, args.steps)
+    frames = sum(s.frames for s in specs)
+    px = sum(s.frames * s.height * s.width for s in specs)
+    if rank != 0:
+        return
+    peak, kind = peaks()
+    alg = px * 2 + sum(plain_rows) * 80
+    line = {
+        "metric": "batched locate+link frames/s, 64 uneven movies (one graph launch per step)",
+        "value": frames / (batch_ms / 1e3), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": batch_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16 in / f32 compute", "data": "synthetic (rendered on the device)",
+        "config": {"workload": f"{len(specs)} movies, {frames} frames, {px / 1e9:.2f} Gpx u16 "
+                               "(sides 128-2048, aspect 1-2, T 10-500, d 5-11, sep d+1, sr 3-8)",
+                   "movies": len(specs), "frames": frames, "gpx": px / 1e9,
+                   "l2": "inputs larger than L2", "generation_s": gen_s},
+        "plain": {"value": frames / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                  "calls_per_step": len(specs)},
+        "batched_over_plain": plain_ms / batch_ms,
+        "roofline": {"bound": "hbm", "kernel": "whole batched step", "achieved": alg / (batch_ms / 1e3) / 1e9,
+                     "peak": peak, "peak_kind": kind, "unit": "GB/s",
+                     "frac": alg / (batch_ms / 1e3) / 1e9 / peak, "traffic": None, "algorithmic_bytes": alg},
+        "batch_stats": {"graph": stats[-1]["batch_graph"], "launches": stats[-1]["launches"],
+                        "link_passes": stats[-1]["link_iterations"], "fallbacks": stats[-1]["batch_fallbacks"],
+                        "rows": sum(plain_rows)},
+        "gpu_launches": int(sum(x["launches"] for x in stats)),
+        "e2e": None,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -314,7 +417,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="locate-link", choices=["locate-link", "adjoint"])
+    ap.add_argument("--workload", default="locate-link", choices=["locate-link", "adjoint", "batched"])
     ap.add_argument("--frames", type=int, default=None,
                     help="smaller movie of the same spot model (profiling captures only)")
     args = ap.parse_args()
@@ -326,6 +429,9 @@ def main():
         return
     if args.workload == "adjoint":
         run_adjoint(args, rank, world, local)
+        return
+    if args.workload == "batched":
+        run_batched(args, rank, world, local)
         return
 
     import torch

@@ -126,6 +126,31 @@ GT_API int gt_batch_device(gt_ctx* ctx, const void* d_frames, int dtype, int T, 
                     const gt_params* params, float* d_out, int64_t out_rows,
                     int64_t* nrows, void* stream);
 
+/* One movie of a batched call (gt_batch_many_device): device-resident
+ * frames with their own shape, dtype and parameters, and the device buffer
+ * that receives the movie's gt_batch_device table. */
+typedef struct gt_movie {
+    const void* frames;   /* T x H x W, u16 or f32, device */
+    int32_t dtype;        /* gt_dtype */
+    int32_t T, H, W;
+    gt_params params;
+    float* out;           /* out_rows x ncols f32, device (rows beyond are dropped) */
+    int64_t out_rows;
+    int64_t nrows;        /* written: rows of the movie's table */
+} gt_movie;
+
+/* Locate (and link) n movies of uneven sizes and parameters in one CUDA
+ * graph launch on `stream`: the movies' locate / ordering / output kernels
+ * run as parallel graph branches and all linking runs in one cooperative
+ * kernel over every movie.  The graph is built on the first call and
+ * replayed while the movies' pointers, shapes and parameters stay the same.
+ * Tile rows of the specialised locate kernel are chosen per (frame size,
+ * diameter) by timing both variants once per context.  A movie whose
+ * per-frame capacities overflow is rerun through the gt_batch_device path.
+ * Each movie's table equals what gt_batch_device returns for it.  No
+ * reference counterpart (the reference processes one movie per call). */
+GT_API int gt_batch_many_device(gt_ctx* ctx, gt_movie* movies, int n, void* stream);
+
 /* gt_batch_device that also writes, for each output row r < out_rows, the
  * walk record d_walk[5r .. 5r+4] = {frame, last-read row, last-read column,
  * final row, final column} (int32, device).  The refined position is
@@ -219,6 +244,8 @@ typedef struct gt_stats {
     int32_t link_dirty[8];     /* frames relinked by fixed-point passes 1..8 */
     float ms_adjoint_particles; /* gt_adjoint_*: per-particle kernel */
     float ms_adjoint_dense;     /* gt_adjoint_backward: zeroing + transposed bandpass */
+    int32_t batch_graph;        /* gt_batch_many_device: 2 graph replayed, 1 graph built, 0 no graph */
+    int32_t batch_fallbacks;    /* gt_batch_many_device: movies rerun through gt_batch_device */
 } gt_stats;
 
 GT_API int gt_last_stats(const gt_ctx* ctx, gt_stats* out);

@@ -14,7 +14,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared():
-    src = open(os.path.join(ROOT, "include", "gt.h")).read()
+    inc = os.path.join(ROOT, "include")
+    src = "".join(open(os.path.join(inc, h)).read() for h in sorted(os.listdir(inc)) if h.endswith(".h"))
     return sorted(set(re.findall(r"GT_API\s+[\w\s\*]*?\b(gt_\w+)\s*\(", src)))
 
 
@@ -92,8 +93,9 @@ def test_struct_layouts_match_header(tmp_path):
 #include <stddef.h>
 #include "gt.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(gt_params), sizeof(gt_table), sizeof(gt_stats),
-         offsetof(gt_params, gap_radius), offsetof(gt_table, names), offsetof(gt_stats, ms_total));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(gt_params), sizeof(gt_table), sizeof(gt_stats),
+         offsetof(gt_params, gap_radius), offsetof(gt_table, names), offsetof(gt_stats, ms_total),
+         sizeof(gt_movie), offsetof(gt_movie, params), offsetof(gt_movie, out), offsetof(gt_stats, batch_fallbacks));
   return 0;
 }
 """)
@@ -101,7 +103,9 @@ int main(void) {
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [ctypes.sizeof(_native.GtParams), ctypes.sizeof(_native.GtTable), ctypes.sizeof(_native.GtStats),
-            _native.GtParams.gap_radius.offset, _native.GtTable.names.offset, _native.GtStats.ms_total.offset]
+            _native.GtParams.gap_radius.offset, _native.GtTable.names.offset, _native.GtStats.ms_total.offset,
+            ctypes.sizeof(_native.GtMovie), _native.GtMovie.params.offset, _native.GtMovie.out.offset,
+            _native.GtStats.batch_fallbacks.offset]
     assert got == want
 
 

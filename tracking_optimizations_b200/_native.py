@@ -78,6 +78,22 @@ class GtStats(ctypes.Structure):
         ("link_dirty", ctypes.c_int32 * 8),
         ("ms_adjoint_particles", ctypes.c_float),
         ("ms_adjoint_dense", ctypes.c_float),
+        ("batch_graph", ctypes.c_int32),
+        ("batch_fallbacks", ctypes.c_int32),
+    ]
+
+
+class GtMovie(ctypes.Structure):
+    _fields_ = [
+        ("frames", ctypes.c_void_p),
+        ("dtype", ctypes.c_int32),
+        ("T", ctypes.c_int32),
+        ("H", ctypes.c_int32),
+        ("W", ctypes.c_int32),
+        ("params", GtParams),
+        ("out", ctypes.c_void_p),
+        ("out_rows", ctypes.c_int64),
+        ("nrows", ctypes.c_int64),
     ]
 
 
@@ -105,6 +121,11 @@ SIGNATURES = [
                                             ctypes.c_int, ctypes.c_int, ctypes.POINTER(GtParams), ctypes.c_void_p,
                                             ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p,
                                             ctypes.c_void_p]),
+    ("gt_batch_many_device", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GtMovie), ctypes.c_int,
+                                            ctypes.c_void_p]),
+    ("gt_synth_render", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_uint64,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     ("gt_adjoint_forward", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.POINTER(GtParams), ctypes.c_void_p, ctypes.c_int64,
                                           ctypes.c_void_p, ctypes.c_void_p]),

@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgt.so")
 SOURCES = ["gt_api.cu", "locate.cu", "locate_fast.cu", "finalize.cu", "link.cu", "assemble.cu", "noalloc.cu",
-           "adjoint.cu"]
+           "adjoint.cu", "synth.cu"]
 
 # --fmad=false: the only fused multiply-adds are explicit fmaf() calls, so the
 # kernels reproduce the oracle's operation order bit for bit.
@@ -33,7 +33,7 @@ def nvcc():
 def build(force=False, verbose=False):
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     hdrs = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
-    hdrs.append(os.path.join(ROOT, "include", "gt.h"))
+    hdrs += [os.path.join(ROOT, "include", h) for h in os.listdir(os.path.join(ROOT, "include")) if h.endswith(".h")]
     if not force and os.path.exists(LIB):
         t = os.path.getmtime(LIB)
         if all(os.path.getmtime(s) <= t for s in srcs + hdrs):

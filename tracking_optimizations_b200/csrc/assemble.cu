@@ -59,6 +59,7 @@ __global__ void assemble_kernel(AsmArgs a) {
     const size_t fbase = (size_t)t * a.H * a.W;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int g = a.off[t] + i;
+        if (g >= a.out_rows) break;  // rows in index order: the rest are beyond too
         const size_t s = (size_t)t * a.cap_p + i;
         float* row = a.out + (size_t)g * a.ncols;
         const float mass = a.pm[s];

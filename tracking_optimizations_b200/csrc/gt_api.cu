@@ -6,6 +6,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <array>
+#include <climits>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -40,6 +42,8 @@ cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* 
                                      const int* circ, const float* grad, float* yxm, float* gR, double* gpar,
                                      int* err, int num_sms, cudaStream_t st);
 cudaError_t launch_adjoint_transpose(const AdjParams& p, const float* gR, float* gI, cudaStream_t st);
+__global__ void link_fixpoint_multi_kernel(const LinkBufs* Ls, const int* memory, const int* fstart, int nm,
+                                           int max_passes, int* ndirty, int* passes);
 }  // namespace gt
 
 using namespace gt;
@@ -57,6 +61,16 @@ struct gt_ctx {
     unsigned int* d_count = nullptr;
     int force_generic = 0;            // always use locate_tiles_kernel
     int fast_tile_rows = 32;          // output tile height of the fast kernel (32 or 64)
+    // batched path (gt_batch_many_device)
+    std::map<std::array<int, 6>, int> tile_rows;  // autotuned tile rows per (H, W, krad, D, rc, dtype)
+    std::string batch_key;            // inputs of the cached graph
+    cudaGraphExec_t batch_exec = nullptr;
+    cudaStream_t side[8] = {};
+    cudaEvent_t bev[20] = {};         // fork/join events
+    int* h_status = nullptr;          // pinned: 8 ints per movie
+    size_t h_status_n = 0;
+    int tune_disabled = 0;
+    int batch_cap_div = 64;           // first candidate capacity of batched movies: H*W / this
 };
 
 namespace {
@@ -209,7 +223,7 @@ void annulus_inds_f(float outer, float inner, std::vector<int>& off) {
 }
 
 int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int num_sms, Plan* pl,
-              std::string* msg, int force_generic_flag = 0, int fast_tile_rows = 32) {
+              std::string* msg, int force_generic_flag = 0, int fast_tile_rows = 32, int cap_div = 64) {
     Plan& P = *pl;
     P.T = T; P.H = H; P.W = W; P.dtype = dtype; P.r = r;
     LocParams& lp = P.lp;
@@ -281,7 +295,7 @@ int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int 
 
     // capacities (bounds; overflow is detected on the device and retried)
     const long long HW = (long long)H * W;
-    long long cc = std::max<long long>(4096, HW / 64) * scale;
+    long long cc = std::max<long long>(4096, HW / cap_div) * scale;
     P.cap_c = (int)std::min<long long>(cc, std::max<long long>(HW, 1));
     const double s = std::max(1.0f, P.sep);
     const double ext_h = H + 2.0 * lp.rint_c + s, ext_w = W + 2.0 * lp.rint_c + s;
@@ -343,7 +357,7 @@ struct Carver {
     }
 };
 
-size_t carve(const Plan& P, char* base, Work* w, size_t frame_bytes, bool need_locate) {
+size_t carve(const Plan& P, char* base, Work* w, size_t frame_bytes, bool need_locate, bool own_out = true) {
     Carver c{base};
     const size_t T = P.T;
     const size_t ncell = (size_t)P.ncx * P.ncy;
@@ -409,7 +423,7 @@ size_t carve(const Plan& P, char* base, Work* w, size_t frame_bytes, bool need_l
     w->bump = c.take<int>(S);
     w->hkey = c.take<int>(S * P.hsize);
     w->hval = c.take<int>(S * P.hsize);
-    w->out = c.take<float>(need_locate ? T * P.cap_p * P.names.size() : 1);
+    w->out = c.take<float>(need_locate && own_out ? T * P.cap_p * P.names.size() : 1);
     return c.off + 256;
 }
 
@@ -445,6 +459,8 @@ LinkBufs link_bufs(const Plan& P, const Work& w) {
     L.d_cnt = w.d_cnt; L.d_src = w.d_src; L.d_w = w.d_w; L.uf = w.uf; L.c_nd = w.c_nd; L.c_ns = w.c_ns;
     L.c_min = w.c_min; L.vis = w.vis; L.work = w.work; L.bump = w.bump; L.hkey = w.hkey; L.hval = w.hval;
     L.hsize = P.hsize;
+    L.st_s = P.cap_s; L.st_s1 = (long long)P.cap_s + 1; L.st_p1 = (long long)P.cap_p + 1;
+    L.st_n = (long long)P.cap_s + P.cap_p; L.st_e = P.cap_e; L.st_h = P.hsize;
     return L;
 }
 
@@ -613,6 +629,7 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
     a.sig_off = w.sig_off; a.n_sig = (int)P.sig_off.size() / 2;
     a.bg_off = w.bg_off; a.n_bg = (int)P.bg_off.size() / 2;
     a.out = w.out;
+    a.out_rows = LLONG_MAX;
     a.walk = d_walk;
     a.walk_rows = walk_rows;
     assemble_kernel<<<T, 256, 0, st>>>(a);
@@ -744,6 +761,477 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
     return GT_ERR_CAPACITY;
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched uneven movies (gt_batch_many_device).
+//
+// Every movie gets its own plan and workspace in one arena.  The locate,
+// fallback, ordering/separation and output kernels of the movies are
+// enqueued on side streams (parallel graph branches), the linking of all
+// movies runs in one cooperative kernel (link_fixpoint_multi_kernel) whose
+// blocks share one scratch pool, and the sequence is captured once into a
+// CUDA graph that is replayed while the inputs stay the same.
+// ---------------------------------------------------------------------------
+
+struct BatchMovie {
+    Plan P;
+    Work w;
+    size_t off = 0;
+    bool fast = false;
+    FixedDiv dn{}, dk{};
+    int link_slot = -1;  // index among the linked movies
+};
+
+struct BatchShared {
+    LinkBufs* d_L = nullptr;
+    int* d_mem = nullptr;
+    int* d_fstart = nullptr;
+    int* d_ndirty = nullptr;
+    int* d_passes = nullptr;
+    int* d_status = nullptr;  // 8 ints per movie: err[0..3], nrows
+    int nlink = 0, max_passes = 0, link_grid = 0;
+    int launches = 0;
+};
+
+// Tile rows of the specialised locate kernel for one (frame size, diameter)
+// class: both variants timed on up to 32 frames of the movie, the faster
+// kept for the context's lifetime.
+int tune_tile_rows(gt_ctx* ctx, BatchMovie& bm, const void* frames, cudaStream_t st) {
+    Plan& P = bm.P;
+    const std::array<int, 6> key{P.H, P.W, P.lp.krad, P.lp.D, P.lp.rint_c, P.dtype};
+    auto it = ctx->tile_rows.find(key);
+    int best = 32;
+    if (it != ctx->tile_rows.end()) {
+        best = it->second;
+    } else if (!ctx->tune_disabled) {
+        for (int i = 0; i < 2; ++i)
+            if (!ctx->ev[i]) CK(cudaEventCreate(&ctx->ev[i]));
+        const int nf = std::min(P.T, 32);
+        float ms[2] = {0.f, 0.f};
+        const int ths[2] = {32, 64};
+        for (int v = 0; v < 2; ++v) {
+            Plan Q;
+            std::string msg;
+            if (make_plan(P.r, P.T, P.H, P.W, P.dtype, 1, ctx->num_sms, &Q, &msg, 0, ths[v])) return GT_ERR_ARG;
+            MovieBufs b = movie_bufs(Q, bm.w, frames);
+            const int ntiles = Q.lp.ntx * Q.lp.nty;
+            for (int rep = 0; rep < 2; ++rep) {
+                CK(cudaMemsetAsync(bm.w.fcount, 0, sizeof(int) * P.T, st));
+                CK(cudaMemsetAsync(bm.w.npend, 0, sizeof(int), st));
+                CK(cudaMemsetAsync(bm.w.err, 0, sizeof(int) * 4, st));
+                CK(cudaEventRecord(ctx->ev[0], st));
+                int used_tma = 0;
+                CK(launch_locate_fast(Q.lp.krad, Q.lp.D, Q.lp.rint_c, ths[v], dim3(ntiles, nf), st, Q.lp, b, bm.dn,
+                                      bm.dk, P.T, 0, &used_tma));
+                CK(cudaEventRecord(ctx->ev[1], st));
+                CK(cudaEventSynchronize(ctx->ev[1]));
+                CK(cudaEventElapsedTime(&ms[v], ctx->ev[0], ctx->ev[1]));
+            }
+        }
+        best = ms[1] < ms[0] ? 64 : 32;
+        ctx->tile_rows[key] = best;
+    }
+    if (best != P.fast_th) {
+        Plan Q;
+        std::string msg;
+        if (make_plan(P.r, P.T, P.H, P.W, P.dtype, 1, ctx->num_sms, &Q, &msg, 0, best)) return GT_ERR_ARG;
+        Work w2{};
+        Plan Qc = Q, Pc = P;
+        Qc.nslot = 0;
+        Pc.nslot = 0;
+        if (carve(Qc, nullptr, &w2, 0, true, false) == carve(Pc, nullptr, &w2, 0, true, false)) P = Q;
+    }
+    return GT_OK;
+}
+
+// Locate, fallback walks, ordering + separation filter and frame offsets of
+// one movie (the front half of run_pipeline, without host synchronisation).
+int enqueue_front(gt_ctx* ctx, BatchMovie& bm, const void* frames, cudaStream_t s, int* launches) {
+    const Plan& P = bm.P;
+    const Work& w = bm.w;
+    const int T = P.T;
+    MovieBufs b = movie_bufs(P, w, frames);
+    CK(cudaMemsetAsync(w.fcount, 0, sizeof(int) * T, s));
+    CK(cudaMemsetAsync(w.npend, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(w.err, 0, sizeof(int) * 4, s));
+    const int ntiles = P.lp.ntx * P.lp.nty;
+    if (bm.fast) {
+        for (int f0 = 0; f0 < T; f0 += 65535) {
+            int used_tma = 0;
+            CK(launch_locate_fast(P.lp.krad, P.lp.D, P.lp.rint_c, P.fast_th, dim3(ntiles, std::min(65535, T - f0)), s,
+                                  P.lp, b, bm.dn, bm.dk, T, f0, &used_tma));
+            ++*launches;
+        }
+    } else {
+        LocParams lg = P.lp;
+        lg.TH = LOC_TH;
+        lg.TW = LOC_TW;
+        lg.ntx = (P.W + LOC_TW - 1) / LOC_TW;
+        lg.nty = (P.H + LOC_TH - 1) / LOC_TH;
+        for (int f0 = 0; f0 < T; f0 += 65535) {
+            dim3 grid(lg.ntx * lg.nty, std::min(65535, T - f0));
+            locate_tiles_kernel<<<grid, 256, P.smem_loc, s>>>(lg, b, f0);
+            ++*launches;
+        }
+    }
+    CK(cudaGetLastError());
+    fallback_walk_kernel<<<ctx->num_sms, 128, P.smem_fb, s>>>(P.lp, b, P.fb_win);
+    finalize_kernel<<<T, 512, P.smem_fin, s>>>(P.lp, b, P.sep, P.link);
+    scan_frames_kernel<<<1, 1024, 0, s>>>(w.npart, w.off, T);
+    CK(cudaGetLastError());
+    *launches += 3;
+    if (P.link) {
+        CK(cudaMemsetAsync(w.mcount, 0, sizeof(int) * T, s));
+        CK(cudaMemsetAsync(w.dirty, 0, sizeof(int) * T, s));
+    }
+    return GT_OK;
+}
+
+// Trajectory ids and the output table of one movie, then its status words.
+int enqueue_back(gt_ctx* ctx, BatchMovie& bm, const gt_movie& mv, int* d_status, cudaStream_t s, int* launches) {
+    const Plan& P = bm.P;
+    const Work& w = bm.w;
+    const int T = P.T;
+    if (P.link) {
+        scan_frames_kernel<<<1, 1024, 0, s>>>(w.newcount, w.newbase, T);
+        newid_kernel<<<T, 256, 0, s>>>(w.newrank, w.newbase, w.off, w.npart, w.newid, T);
+        *launches += 2;
+    }
+    AsmArgs a{};
+    a.T = T; a.H = P.H; a.W = P.W; a.cap_p = P.cap_p; a.cap_c = P.cap_c; a.ncols = (int)P.names.size();
+    a.has_link = P.link; a.cpu_processed = P.r.cpu_processed; a.characterize = P.r.characterize;
+    a.sig = P.r.has_sig; a.bg = P.r.has_bg;
+    a.frames = mv.frames; a.dtype = P.dtype;
+    a.py = w.py; a.px = w.px; a.pm = w.pm; a.prec = w.prec; a.npart = w.npart; a.off = w.off;
+    a.cand = w.cand; a.root = w.root; a.newid = w.newid;
+    a.sig_off = w.sig_off; a.n_sig = (int)P.sig_off.size() / 2;
+    a.bg_off = w.bg_off; a.n_bg = (int)P.bg_off.size() / 2;
+    a.out = mv.out;
+    a.out_rows = mv.out ? mv.out_rows : 0;
+    assemble_kernel<<<T, 256, 0, s>>>(a);
+    CK(cudaGetLastError());
+    *launches += 1;
+    CK(cudaMemcpyAsync(d_status, w.err, sizeof(int) * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(d_status + 4, w.off + T, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    return GT_OK;
+}
+
+// The whole batch on `st`, fanned out over the context's side streams.
+int enqueue_batch(gt_ctx* ctx, std::vector<BatchMovie>& B, gt_movie* mv, int n, BatchShared& S, cudaStream_t st) {
+    const int K = 8;
+    S.launches = 0;
+    CK(cudaEventRecord(ctx->bev[0], st));
+    for (int k = 0; k < K; ++k) CK(cudaStreamWaitEvent(ctx->side[k], ctx->bev[0], 0));
+    for (int i = 0; i < n; ++i) {
+        int rc = enqueue_front(ctx, B[i], mv[i].frames, ctx->side[i % K], &S.launches);
+        if (rc) return rc;
+    }
+    for (int k = 0; k < K; ++k) {
+        CK(cudaEventRecord(ctx->bev[1 + k], ctx->side[k]));
+        CK(cudaStreamWaitEvent(st, ctx->bev[1 + k], 0));
+    }
+    if (S.nlink > 0) {
+        CK(cudaMemsetAsync(S.d_ndirty, 0, sizeof(int) * (S.max_passes + 2), st));
+        const LinkBufs* Ls = S.d_L;
+        const int* mem = S.d_mem;
+        const int* fst = S.d_fstart;
+        int nm = S.nlink, mp = S.max_passes;
+        int* nd = S.d_ndirty;
+        int* ps = S.d_passes;
+        void* args[] = {(void*)&Ls, (void*)&mem, (void*)&fst, &nm, &mp, &nd, &ps};
+        CK(cudaLaunchCooperativeKernel((const void*)link_fixpoint_multi_kernel, dim3(S.link_grid), dim3(256), args,
+                                       96 * 1024, st));
+        S.launches += 1;
+    }
+    CK(cudaEventRecord(ctx->bev[9], st));
+    for (int k = 0; k < K; ++k) CK(cudaStreamWaitEvent(ctx->side[k], ctx->bev[9], 0));
+    for (int i = 0; i < n; ++i) {
+        int rc = enqueue_back(ctx, B[i], mv[i], S.d_status + 8 * i, ctx->side[i % K], &S.launches);
+        if (rc) return rc;
+    }
+    for (int k = 0; k < K; ++k) {
+        CK(cudaEventRecord(ctx->bev[10 + k], ctx->side[k]));
+        CK(cudaStreamWaitEvent(st, ctx->bev[10 + k], 0));
+    }
+    CK(cudaMemcpyAsync(ctx->h_status, S.d_status, sizeof(int) * 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    return GT_OK;
+}
+
+int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
+    if (!ctx) return GT_ERR_ARG;
+    ctx->err.clear();
+    ctx->stats = gt_stats{};
+    if (n < 0 || (n > 0 && !mv)) { ctx->err = "invalid movie list"; return GT_ERR_ARG; }
+    if (n == 0) return GT_OK;
+    CK(cudaSetDevice(ctx->device));
+    std::vector<BatchMovie> B(n);
+    std::string key;
+    for (int i = 0; i < n; ++i) {
+        const gt_movie& m = mv[i];
+        const std::string who = "movie " + std::to_string(i) + ": ";
+        if (!m.frames || m.T < 1 || m.H < 1 || m.W < 1 || (m.dtype != GT_U16 && m.dtype != GT_F32) ||
+            (m.out_rows > 0 && !m.out) || m.out_rows < 0) {
+            ctx->err = who + "invalid frames/shape/dtype/output";
+            return GT_ERR_ARG;
+        }
+        if ((long long)m.H * m.W > (1LL << 28) || m.H > 65535 || m.W > 65535) {
+            ctx->err = who + "frame too large";
+            return GT_ERR_ARG;
+        }
+        Resolved r;
+        std::string msg;
+        int rc = resolve(&m.params, &r, &msg);
+        if (rc) { ctx->err = who + msg; return rc; }
+        rc = make_plan(r, m.T, m.H, m.W, m.dtype, 1, ctx->num_sms, &B[i].P, &msg, ctx->force_generic, 32,
+                       ctx->batch_cap_div);
+        if (rc) { ctx->err = who + msg; return rc; }
+        char buf[128];
+        std::snprintf(buf, sizeof(buf), "%p|%d|%d|%d|%d|%p|%lld|", m.frames, m.dtype, m.T, m.H, m.W, (void*)m.out,
+                      (long long)m.out_rows);
+        key += buf;
+        key.append((const char*)&m.params, sizeof(gt_params));
+    }
+    // pinned status words, side streams, events
+    if (ctx->h_status_n < (size_t)8 * n) {
+        if (ctx->h_status) cudaFreeHost(ctx->h_status);
+        ctx->h_status = nullptr;
+        ctx->h_status_n = 0;
+        CK(cudaHostAlloc((void**)&ctx->h_status, sizeof(int) * 8 * (size_t)n, cudaHostAllocDefault));
+        ctx->h_status_n = (size_t)8 * n;
+    }
+    for (auto& sd : ctx->side)
+        if (!sd) CK(cudaStreamCreateWithFlags(&sd, cudaStreamNonBlocking));
+    for (auto& e : ctx->bev)
+        if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (int i = 0; i < 5; ++i)
+        if (!ctx->ev[i]) CK(cudaEventCreate(&ctx->ev[i]));
+    // division checks and kernel choice (host-synchronous, before any capture)
+    for (int i = 0; i < n; ++i) {
+        BatchMovie& bm = B[i];
+        bm.fast = bm.P.fast != 0;
+        if (bm.fast) {
+            bool ok = false;
+            int rc = fast_division(ctx, bm.P, &bm.dn, &bm.dk, &ok, st);
+            if (rc) return rc;
+            bm.fast = ok;
+        }
+    }
+    // linked movies: shared slot strides
+    BatchShared S;
+    long long st_s = 1, st_s1 = 1, st_p1 = 1, st_n = 1, st_e = 1, st_h = 64;
+    for (int i = 0; i < n; ++i) {
+        const Plan& P = B[i].P;
+        if (!P.link) continue;
+        B[i].link_slot = S.nlink++;
+        st_s = std::max<long long>(st_s, P.cap_s);
+        st_s1 = std::max<long long>(st_s1, (long long)P.cap_s + 1);
+        st_p1 = std::max<long long>(st_p1, (long long)P.cap_p + 1);
+        st_n = std::max<long long>(st_n, (long long)P.cap_s + P.cap_p);
+        st_e = std::max<long long>(st_e, P.cap_e);
+        st_h = std::max<long long>(st_h, P.hsize);
+        S.max_passes = std::max(S.max_passes, P.T + 1);
+    }
+    if (S.nlink > 0) {
+        CK(cudaFuncSetAttribute(link_fixpoint_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_multi_kernel, 256, 96 * 1024));
+        const size_t per_slot = 4 * (3 * st_s + st_s1) + 8 * st_e * 2 + 4 * st_p1 + 4 * 4 * st_n + st_n + 16 * st_n +
+                                4 + 8 * st_h;
+        const size_t budget = (size_t)6 << 30;
+        S.link_grid = (int)std::max<size_t>(1, std::min<size_t>((size_t)per_sm * ctx->num_sms, budget / per_slot));
+    }
+    // arena layout: movies, link pool, shared arrays
+    size_t total = 0;
+    for (int i = 0; i < n; ++i) {
+        Plan Pc = B[i].P;
+        Pc.nslot = 0;
+        Work w{};
+        B[i].off = total;
+        total += carve(Pc, nullptr, &w, 0, true, false);
+        total = (total + 255) / 256 * 256;
+    }
+    const size_t G = S.link_grid;
+    Carver pc{nullptr};
+    auto pool_layout = [&](Carver& c, Work& pw) {
+        pw.s_y = c.take<float>(G * st_s); pw.s_x = c.take<float>(G * st_s); pw.s_h = c.take<int>(G * st_s);
+        pw.s_deg = c.take<int>(G * st_s1); pw.e_dst = c.take<int>(G * st_e); pw.e_w = c.take<float>(G * st_e);
+        pw.d_cnt = c.take<int>(G * st_p1); pw.d_src = c.take<int>(G * st_e); pw.d_w = c.take<float>(G * st_e);
+        pw.uf = c.take<int>(G * st_n); pw.c_nd = c.take<int>(G * st_n); pw.c_ns = c.take<int>(G * st_n);
+        pw.c_min = c.take<int>(G * st_n); pw.vis = c.take<unsigned char>(G * st_n);
+        pw.work = c.take<int>(G * 4 * st_n); pw.bump = c.take<int>(G); pw.hkey = c.take<int>(G * st_h);
+        pw.hval = c.take<int>(G * st_h);
+        S.d_L = c.take<LinkBufs>(std::max(1, S.nlink));
+        S.d_mem = c.take<int>(std::max(1, S.nlink));
+        S.d_fstart = c.take<int>(std::max(1, S.nlink));
+        S.d_ndirty = c.take<int>(S.max_passes + 2);
+        S.d_passes = c.take<int>(1);
+        S.d_status = c.take<int>(8 * (size_t)n);
+    };
+    Work pool{};
+    pool_layout(pc, pool);
+    const size_t pool_bytes = pc.off + 256;
+    const size_t need = total + pool_bytes;
+    {
+        // the batch must fit beside the caller's data: tighter first
+        // candidate capacities (overflowing movies are rerun alone)
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t avail = free_b + (ctx->arena ? ctx->arena_size : 0);
+        if (need > avail - avail / 8) {
+            if (ctx->batch_cap_div < 1024) {
+                ctx->batch_cap_div *= 4;
+                const int rc2 = batch_many(ctx, mv, n, st);
+                ctx->batch_cap_div = 64;
+                return rc2;
+            }
+            ctx->err = "the batch does not fit in device memory; split it";
+            return GT_ERR_OOM;
+        }
+    }
+    int rc = ensure_arena(ctx, need);
+    if (rc) return rc;
+    {
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), "arena %p %p %d %d %d", (void*)ctx->arena, (void*)st, ctx->force_generic,
+                      ctx->tune_disabled, ctx->batch_cap_div);
+        key += buf;
+    }
+    for (int i = 0; i < n; ++i) {
+        Plan Pc = B[i].P;
+        Pc.nslot = 0;
+        carve(Pc, ctx->arena + B[i].off, &B[i].w, 0, true, false);
+    }
+    Carver c2{ctx->arena + total};
+    pool_layout(c2, pool);
+    const bool replay = ctx->batch_exec && key == ctx->batch_key;
+    // constant tables and linker descriptors (other calls may have reused
+    // the arena since the graph was built)
+    for (int i = 0; i < n; ++i) {
+        rc = upload_tables(ctx, B[i].P, B[i].w, st);
+        if (rc) return rc;
+    }
+    std::vector<LinkBufs> hL(std::max(1, S.nlink));
+    std::vector<int> hm(std::max(1, S.nlink)), hf(std::max(1, S.nlink));
+    if (S.nlink > 0) {
+        int fs = 0;
+        for (int i = 0; i < n; ++i) {
+            if (B[i].link_slot < 0) continue;
+            LinkBufs L = link_bufs(B[i].P, B[i].w);
+            L.nslot = (int)G;
+            L.s_y = pool.s_y; L.s_x = pool.s_x; L.s_h = pool.s_h; L.s_deg = pool.s_deg;
+            L.e_dst = pool.e_dst; L.e_w = pool.e_w; L.d_cnt = pool.d_cnt; L.d_src = pool.d_src; L.d_w = pool.d_w;
+            L.uf = pool.uf; L.c_nd = pool.c_nd; L.c_ns = pool.c_ns; L.c_min = pool.c_min; L.vis = pool.vis;
+            L.work = pool.work; L.bump = pool.bump; L.hkey = pool.hkey; L.hval = pool.hval;
+            L.st_s = st_s; L.st_s1 = st_s1; L.st_p1 = st_p1; L.st_n = st_n; L.st_e = st_e; L.st_h = st_h;
+            L.lsm_bytes = 96 * 1024;
+            hL[B[i].link_slot] = L;
+            hm[B[i].link_slot] = (int)B[i].P.r.memory;
+            hf[B[i].link_slot] = fs;
+            fs += B[i].P.T;
+        }
+        CK(cudaMemcpyAsync(S.d_L, hL.data(), sizeof(LinkBufs) * S.nlink, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.d_mem, hm.data(), sizeof(int) * S.nlink, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.d_fstart, hf.data(), sizeof(int) * S.nlink, cudaMemcpyHostToDevice, st));
+    }
+    if (!replay) {
+        if (ctx->batch_exec) { cudaGraphExecDestroy(ctx->batch_exec); ctx->batch_exec = nullptr; }
+        ctx->batch_key.clear();
+        // autotuned tile rows (timed on this movie's frames and workspace)
+        for (int i = 0; i < n; ++i)
+            if (B[i].fast) {
+                rc = tune_tile_rows(ctx, B[i], mv[i].frames, st);
+                if (rc) return rc;
+            }
+        size_t sl = 0, sf = 0, sn = 0;
+        for (int i = 0; i < n; ++i) {
+            sl = std::max(sl, B[i].P.smem_loc);
+            sf = std::max(sf, B[i].P.smem_fb);
+            sn = std::max(sn, B[i].P.smem_fin);
+        }
+        CK(cudaFuncSetAttribute(locate_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sl));
+        CK(cudaFuncSetAttribute(fallback_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf));
+        CK(cudaFuncSetAttribute(finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sn));
+        CK(cudaStreamSynchronize(st));
+        // capture; where capture is refused, run the same sequence directly
+        cudaGraph_t graph = nullptr;
+        bool captured = false;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+            const int erc = enqueue_batch(ctx, B, mv, n, S, st);
+            const cudaError_t ee = cudaStreamEndCapture(st, &graph);
+            if (erc == GT_OK && ee == cudaSuccess && graph) {
+                cudaGraphExec_t ex = nullptr;
+                if (cudaGraphInstantiate(&ex, graph, 0) == cudaSuccess) {
+                    ctx->batch_exec = ex;
+                    ctx->batch_key = key;
+                    captured = true;
+                }
+            }
+            if (graph) cudaGraphDestroy(graph);
+            if (!captured) {
+                cudaGetLastError();
+                ctx->err.clear();
+            }
+        } else {
+            cudaGetLastError();
+        }
+        CK(cudaEventRecord(ctx->ev[0], st));
+        if (captured) {
+            CK(cudaGraphLaunch(ctx->batch_exec, st));
+            ctx->stats.batch_graph = 1;
+        } else {
+            rc = enqueue_batch(ctx, B, mv, n, S, st);
+            if (rc) return rc;
+        }
+    } else {
+        CK(cudaStreamSynchronize(st));
+        CK(cudaEventRecord(ctx->ev[0], st));
+        CK(cudaGraphLaunch(ctx->batch_exec, st));
+        ctx->stats.batch_graph = 2;
+        // launches of the captured sequence
+        int cnt = 0;
+        for (int i = 0; i < n; ++i) {
+            const Plan& P = B[i].P;
+            cnt += (P.T + 65534) / 65535 + 3 + (P.link ? 2 : 0) + 1;
+        }
+        S.launches = cnt + (S.nlink > 0 ? 1 : 0);
+    }
+    CK(cudaEventRecord(ctx->ev[1], st));
+    CK(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&ctx->stats.ms_total, ctx->ev[0], ctx->ev[1]);
+    ctx->stats.launches = S.launches;
+    if (S.nlink > 0) {
+        int passes = 0;
+        CK(cudaMemcpy(&passes, S.d_passes, sizeof(int), cudaMemcpyDeviceToHost));
+        ctx->stats.link_iterations = passes;
+    }
+    // per-movie status; capacity overflows are rerun through the plain path
+    std::vector<int> status(ctx->h_status, ctx->h_status + 8 * (size_t)n);
+    gt_stats keep = ctx->stats;
+    int fallbacks = 0;
+    int64_t rows_total = 0;
+    for (int i = 0; i < n; ++i) {
+        const int bits = status[8 * i];
+        bool retry = false;
+        rc = err_status(ctx, bits, &retry);
+        if (rc && !retry) { ctx->err = "movie " + std::to_string(i) + ": " + ctx->err; return rc; }
+        if (rc && retry) {
+            ++fallbacks;
+            int64_t nr = 0;
+            rc = batch_common(ctx, mv[i].frames, false, mv[i].dtype, mv[i].T, mv[i].H, mv[i].W, &mv[i].params,
+                              nullptr, mv[i].out, mv[i].out_rows, &nr, st);
+            if (rc) { ctx->err = "movie " + std::to_string(i) + ": " + ctx->err; return rc; }
+            mv[i].nrows = nr;
+        } else {
+            mv[i].nrows = status[8 * i + 4];
+        }
+        rows_total += mv[i].nrows;
+    }
+    ctx->err.clear();
+    ctx->stats = keep;
+    ctx->stats.batch_fallbacks = fallbacks;
+    ctx->stats.particles = rows_total;
+    return GT_OK;
+}
 
 // Parameters of the gt_adjoint_* calls: the forward weights exactly as
 // make_plan derives them, the normalised taps a_i = w_i / sum(w) and
@@ -886,6 +1374,12 @@ void gt_ctx_destroy(gt_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->arena) cudaFree(ctx->arena);
     if (ctx->d_count) cudaFree(ctx->d_count);
+    if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    for (auto& sd : ctx->side)
+        if (sd) cudaStreamDestroy(sd);
+    for (auto& e : ctx->bev)
+        if (e) cudaEventDestroy(e);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1028,11 +1522,17 @@ int gt_adjoint_uncertainty(gt_ctx* ctx, const float* d_frames, int T, int H, int
     return rc;
 }
 
+int gt_batch_many_device(gt_ctx* ctx, gt_movie* movies, int n, void* stream) {
+    cudaStream_t st = stream ? (cudaStream_t)stream : (ctx ? ctx->stream : nullptr);
+    return batch_many(ctx, movies, n, st);
+}
+
 int gt_ctx_set_option(gt_ctx* ctx, const char* key, int value) {
     if (!ctx || !key) return GT_ERR_ARG;
     const std::string k(key);
     if (k == "locate_tile_rows" && (value == 32 || value == 64)) { ctx->fast_tile_rows = value; return GT_OK; }
     if (k == "force_generic" && (value == 0 || value == 1)) { ctx->force_generic = value; return GT_OK; }
+    if (k == "autotune" && (value == 0 || value == 1)) { ctx->tune_disabled = !value; return GT_OK; }
     ctx->err = "unknown option or value: " + k;
     return GT_ERR_ARG;
 }

@@ -151,6 +151,9 @@ struct LinkBufs {
     int* hval;
     int hsize;
     int lsm_bytes;        // dynamic shared memory pool of the linker blocks
+    // slot strides of the scratch arrays (>= the capacities above; equal to
+    // the largest movie's when several movies share one pool)
+    long long st_s, st_s1, st_p1, st_n, st_e, st_h;
 };
 
 // Adjoint of bandpass + refine at fixed peaks.  The forward arithmetic uses
@@ -190,6 +193,7 @@ struct AsmArgs {
     const int* bg_off;    // n_bg x {di, dj}, annulus_inds
     int n_bg;
     float* out;
+    long long out_rows;   // rows of `out` (rows beyond are not written)
     int* walk;            // optional n x 5 {frame, last-read row, col, final row, col}
     long long walk_rows;  // rows of `walk` (rows beyond are not written)
 };

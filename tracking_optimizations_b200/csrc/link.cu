@@ -140,20 +140,19 @@ __device__ bool solve_subnet(const LinkBufs& L, const int* dests, int nd, const 
 }  // namespace
 
 // One CTA per frame (grid-stride); frame t >= 1 links P(t-1) + M(t) to P(t).
-__device__ void link_frames_body(const LinkBufs& L, int only_dirty) {
+__device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int tstride) {
     __shared__ int warp_tot[NTL / 32];
     __shared__ int s_total;
     __shared__ int s_bump;
     extern __shared__ __align__(16) int lsm[];  // per-frame scratch pool
     const int slot = blockIdx.x;
-    const int cap_s = L.cap_s, cap_p = L.cap_p;
-    const int nn = cap_s + cap_p;
+    const int cap_p = L.cap_p;
     const float r = L.r;
     const float G = (float)L.G;
     const int ncell = L.ncx * L.ncy;
     const int pool = L.lsm_bytes / 4;
 
-    for (int t = blockIdx.x; t < L.T; t += gridDim.x) {
+    for (int t = t0; t < L.T; t += tstride) {
         if (only_dirty && !__ldcg(L.dirty + t)) continue;
         const int nd = L.npart[t];
         int* pred = L.pred + L.off[t];
@@ -200,17 +199,17 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty) {
                 dx = L.px + (size_t)t * cap_p;
                 gs = L.gstart + (size_t)t * (ncell + 1);
                 gi = L.gidx + (size_t)t * cap_p;
-                sy = L.s_y + (size_t)slot * cap_s;
-                sx = L.s_x + (size_t)slot * cap_s;
-                sh = L.s_h + (size_t)slot * cap_s;
-                sdeg = L.s_deg + (size_t)slot * (cap_s + 1);
-                dcnt = L.d_cnt + (size_t)slot * (cap_p + 1);
-                uf = L.uf + (size_t)slot * nn;
-                cnd = L.c_nd + (size_t)slot * nn;
-                cns = L.c_ns + (size_t)slot * nn;
-                cmin = L.c_min + (size_t)slot * nn;
-                vis = L.vis + (size_t)slot * nn;
-                work = L.work + (size_t)slot * 4 * nn;
+                sy = L.s_y + (size_t)slot * L.st_s;
+                sx = L.s_x + (size_t)slot * L.st_s;
+                sh = L.s_h + (size_t)slot * L.st_s;
+                sdeg = L.s_deg + (size_t)slot * L.st_s1;
+                dcnt = L.d_cnt + (size_t)slot * L.st_p1;
+                uf = L.uf + (size_t)slot * L.st_n;
+                cnd = L.c_nd + (size_t)slot * L.st_n;
+                cns = L.c_ns + (size_t)slot * L.st_n;
+                cmin = L.c_min + (size_t)slot * L.st_n;
+                vis = L.vis + (size_t)slot * L.st_n;
+                work = L.work + (size_t)slot * 4 * L.st_n;
             }
             int* bump = &s_bump;
             if (threadIdx.x == 0) *bump = 0;
@@ -255,10 +254,10 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty) {
             if (sm && need + 4 * ne <= pool) {
                 edst = take(ne); ew = (float*)take(ne); dsrc = take(ne); dw = (float*)take(ne);
             } else {
-                edst = L.e_dst + (size_t)slot * L.cap_e;
-                ew = L.e_w + (size_t)slot * L.cap_e;
-                dsrc = L.d_src + (size_t)slot * L.cap_e;
-                dw = L.d_w + (size_t)slot * L.cap_e;
+                edst = L.e_dst + (size_t)slot * L.st_e;
+                ew = L.e_w + (size_t)slot * L.st_e;
+                dsrc = L.d_src + (size_t)slot * L.st_e;
+                dw = L.d_w + (size_t)slot * L.st_e;
             }
             if (ne > L.cap_e) {
                 if (threadIdx.x == 0) atomicOr(L.err, ERR_EDGE_OVERFLOW);
@@ -422,7 +421,7 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty) {
 // linking.rs:479-485, oldest list first, index order within a list),
 // skipping trajectories present in frame t-1 and keeping the first entry of
 // each trajectory.  Marks frames whose M changed.
-__device__ void memory_body(const LinkBufs& L, int memory, int* ndirty) {
+__device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, int tstride) {
     __shared__ int warp_tot[NTL / 32];
     __shared__ int s_total;
     __shared__ int s_diff;
@@ -432,7 +431,7 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty) {
     const int cap_p = L.cap_p;
     const int nn = L.cap_s + cap_p;
     const int pool = L.lsm_bytes / 4;
-    for (int t = blockIdx.x; t < L.T; t += gridDim.x) {
+    for (int t = t0; t < L.T; t += tstride) {
         const int fbeg = max(0, t - 1 - memory), fend = t - 2;
         if (fend < fbeg) continue;
         // number of candidates, to place the scratch
@@ -464,11 +463,11 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty) {
             ch = lsm; cr = ch + cn; cpos = cr + cn; hk = cpos + cn; hv = hk + hs1 + hs2;
             lim = cn;
         } else {
-            ch = L.work + (size_t)slot * 4 * nn;
+            ch = L.work + (size_t)slot * 4 * L.st_n;
             cr = ch + nn;
             cpos = cr + nn;
-            hk = L.hkey + (size_t)slot * L.hsize;
-            hv = L.hval + (size_t)slot * L.hsize;
+            hk = L.hkey + (size_t)slot * L.st_h;
+            hv = L.hval + (size_t)slot * L.st_h;
             lim = nn;
         }
         // candidates in (frame, index) order
@@ -574,14 +573,17 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty) {
 // root[] only ever receives final values, so the walks need no barrier
 // between hops and the result is exact whatever the interleaving; particles
 // of early frames finish first and shorten the later walks.
-__device__ void roots_body(const LinkBufs& L, cg::grid_group& grid) {
+__device__ void roots_reset(const LinkBufs& L) {
     const int n = L.off[L.T];
     const int stride = gridDim.x * blockDim.x;
-    const int g0 = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int g = g0; g < n; g += stride) L.root[g] = -1;
-    grid.sync();
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) L.root[g] = -1;
+}
+
+__device__ void roots_walk(const LinkBufs& L) {
+    const int n = L.off[L.T];
+    const int stride = gridDim.x * blockDim.x;
     volatile int* root = L.root;
-    for (int g = g0; g < n; g += stride) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) {
         int r = g;
         while (true) {
             const int known = root[r];
@@ -592,6 +594,12 @@ __device__ void roots_body(const LinkBufs& L, cg::grid_group& grid) {
         }
         root[g] = r;
     }
+}
+
+__device__ void roots_body(const LinkBufs& L, cg::grid_group& grid) {
+    roots_reset(L);
+    grid.sync();
+    roots_walk(L);
 }
 
 // The whole linker in one cooperative launch: link every frame with M = {},
@@ -614,7 +622,7 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_kernel(LinkBufs L, int m
     cg::grid_group grid = cg::this_grid();
     const bool stamp = blockIdx.x == 0 && threadIdx.x == 0;
     unsigned long long t0 = stamp ? gtimer() : 0, acc[4] = {0, 0, 0, 0};
-    link_frames_body(L, 0);
+    link_frames_body(L, 0, blockIdx.x, gridDim.x);
     int k = 0;
     if (memory > 0 && L.T > 2) {
         for (k = 1; k <= max_passes; ++k) {
@@ -623,11 +631,11 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_kernel(LinkBufs L, int m
             roots_body(L, grid);
             grid.sync();
             if (stamp) { const unsigned long long t = gtimer(); acc[1] += t - t0; t0 = t; }
-            memory_body(L, memory, ndirty + k);
+            memory_body(L, memory, ndirty + k, blockIdx.x, gridDim.x);
             grid.sync();
             if (stamp) { const unsigned long long t = gtimer(); acc[2] += t - t0; t0 = t; }
             if (*(volatile int*)(ndirty + k) == 0) break;
-            link_frames_body(L, 1);
+            link_frames_body(L, 1, blockIdx.x, gridDim.x);
         }
     }
     grid.sync();
@@ -640,6 +648,46 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_kernel(LinkBufs L, int m
         for (int i = 0; i < 4; ++i) phase_ns[i] = acc[i];
     }
     (void)rounds;
+}
+
+// Several movies in one cooperative launch (the batched path): every phase
+// of link_fixpoint_kernel runs over the frames of all movies, movie m's
+// frame t on block (fstart[m] + t) mod gridDim.x so that short movies spread
+// over the grid; one grid barrier per phase serves all movies, and the
+// fixed point ends when no movie's memory entries change.  Ls[m] share one
+// per-block scratch pool (slot strides st_*), since a block links one frame
+// at a time.
+__global__ void __launch_bounds__(NTL, 4) link_fixpoint_multi_kernel(const LinkBufs* Ls, const int* memory,
+                                                                     const int* fstart, int nm, int max_passes,
+                                                                     int* ndirty, int* passes) {
+    cg::grid_group grid = cg::this_grid();
+    const int G = gridDim.x;
+    auto t0_of = [&](int m) { const int s = fstart[m] % G; return ((int)blockIdx.x - s + G) % G; };
+    bool any_mem = false;
+    for (int m = 0; m < nm; ++m) {
+        link_frames_body(Ls[m], 0, t0_of(m), G);
+        any_mem |= memory[m] > 0 && Ls[m].T > 2;
+    }
+    int k = 0;
+    if (any_mem) {
+        for (k = 1; k <= max_passes; ++k) {
+            grid.sync();
+            for (int m = 0; m < nm; ++m) roots_reset(Ls[m]);
+            grid.sync();
+            for (int m = 0; m < nm; ++m) roots_walk(Ls[m]);
+            grid.sync();
+            for (int m = 0; m < nm; ++m)
+                if (memory[m] > 0 && Ls[m].T > 2) memory_body(Ls[m], memory[m], ndirty + k, t0_of(m), G);
+            grid.sync();
+            if (*(volatile int*)(ndirty + k) == 0) break;
+            for (int m = 0; m < nm; ++m) link_frames_body(Ls[m], 1, t0_of(m), G);
+        }
+    }
+    grid.sync();
+    for (int m = 0; m < nm; ++m) roots_reset(Ls[m]);
+    grid.sync();
+    for (int m = 0; m < nm; ++m) roots_walk(Ls[m]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *passes = k;
 }
 
 }  // namespace gt

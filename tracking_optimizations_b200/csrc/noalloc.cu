@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <climits>
 #include <cstring>
 
 #include "gt.h"
@@ -357,6 +358,7 @@ extern "C" int gt_locate_frame_static(const void* d_frame, int dtype, int H, int
     a.root = b.npart; a.newid = b.npart;  // unused without linking
     a.sig_off = d_sig_off; a.n_sig = n_sig; a.bg_off = d_bg_off; a.n_bg = n_bg;
     a.out = stage;
+    a.out_rows = LLONG_MAX;
     assemble_kernel<<<1, 256, 0, st>>>(a);
     SCK(cudaGetLastError());
     int hb[2] = {0, 0};

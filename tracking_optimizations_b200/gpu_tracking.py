@@ -68,6 +68,38 @@ def batch_rust(pyarr, diameter, minmass=None, maxsize=None, separation=None, noi
     return out, cols
 
 
+def batch_device(frames, diameter, **params):
+    """gt_batch_device on a (T, H, W) CUDA tensor (float32, or int16/uint16
+    holding u16 pixels) on the current stream; returns the table as an
+    (n, ncols) float32 CUDA tensor."""
+    import torch
+
+    if not frames.is_cuda or frames.dim() != 3:
+        raise ValueError("frames must be a (T, H, W) CUDA tensor")
+    fr = frames.contiguous()
+    dtype = _native.GT_F32 if fr.dtype == torch.float32 else _native.GT_U16
+    if fr.dtype not in (torch.float32, torch.int16) and not (hasattr(torch, "uint16") and fr.dtype == torch.uint16):
+        raise TypeError("frames must be float32, or int16/uint16 holding u16 pixels")
+    ncols = len(column_names(diameter, **params))
+    p = _native.make_params(diameter, **params)
+    lib = _native.load()
+    index = fr.device.index if fr.device.index is not None else torch.cuda.current_device()
+    ctx = _native.context(index)
+    T, H, W = fr.shape
+    cap = max(1024, T * max(64, H * W // 256))
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for _ in range(2):
+        out = torch.empty((cap, ncols), dtype=torch.float32, device=fr.device)
+        n = ctypes.c_int64()
+        st = lib.gt_batch_device(ctx, ctypes.c_void_p(fr.data_ptr()), dtype, T, H, W, ctypes.byref(p),
+                                 ctypes.c_void_p(out.data_ptr()), cap, ctypes.byref(n), stream)
+        _native.check(st, ctx)
+        if n.value <= cap:
+            return out[: n.value]
+        cap = n.value
+    raise RuntimeError("row count changed between two identical calls")
+
+
 def batch_file_rust(filename, diameter, channel=None, *args, **kwargs):
     """File ingest (TIFF/ETS) is not part of this build's hot path."""
     raise NotImplementedError("batch_file_rust: file ingest is not implemented in the B200 build")

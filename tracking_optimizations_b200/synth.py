@@ -96,3 +96,76 @@ def make_movie(spec, return_truth=False):
     if return_truth:
         return movie, truth, vis
     return movie
+
+
+def batch_workload(n=64, seed=2):
+    """Uneven movies for the batched path: side in {128, 256, 384, 512,
+    1024, 2048}, aspect 1 or 2, T ~ U{10..500}, 0.5-3 spots per 1000 px^2,
+    diameter in {5, 7, 9, 11} with separation = diameter + 1, search_range ~
+    U(3, 8); spot model of PLAIN_1000 (sigma 1.2, A ~ U(150, 1500), step 1.5,
+    Poisson 100 + read noise 5, 2 % blinking).  Parameters the workload
+    leaves open: minmass = 6 d^2 (300 for d = 7, as PLAIN_1000) and memory ~
+    U{0..3}.  About 23 Gpx (47 GB of u16) in total: render with
+    make_movie_device."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    specs = []
+    for i in range(n):
+        side = int(rng.choice([128, 256, 384, 512, 1024, 2048]))
+        aspect = int(rng.choice([1, 2]))
+        H, W = side, side * aspect
+        T = int(rng.integers(10, 501))
+        density = float(rng.uniform(0.5, 3.0))
+        d = int(rng.choice([5, 7, 9, 11]))
+        params = dict(diameter=d, separation=d + 1, minmass=float(6 * d * d),
+                      search_range=float(rng.uniform(3.0, 8.0)), memory=int(rng.integers(0, 4)))
+        specs.append(MovieSpec(T, H, W, max(1, int(round(density * H * W / 1000.0))), 1.2, 150.0, 1500.0, 1.5,
+                               read_noise=5.0, blink=0.02, seed=seed * 1000 + i, params=params))
+    return specs
+
+
+def spot_tracks(spec):
+    """(T, N, 3) float32 (y, x, amplitude) of every spot in every frame, the
+    motion model of make_movie (uniform start, Brownian steps reflected at
+    the borders, amplitude 0 while blinked off), from its own seeded
+    stream."""
+    rng = np.random.Generator(np.random.PCG64(spec.seed))
+    T, H, W, N = spec.frames, spec.height, spec.width, spec.spots
+    pos = np.stack([rng.uniform(0, H - 1, N), rng.uniform(0, W - 1, N)], axis=1)
+    amp = rng.uniform(spec.amp_lo, spec.amp_hi, N)
+    out = np.empty((T, N, 3), np.float32)
+    for t in range(T):
+        on = rng.random(N) >= spec.blink
+        out[t, :, 0] = pos[:, 0]
+        out[t, :, 1] = pos[:, 1]
+        out[t, :, 2] = np.where(on, amp, 0.0)
+        pos = pos + rng.normal(0.0, spec.step, (N, 2))
+        for k, lim in ((0, H - 1), (1, W - 1)):
+            c = pos[:, k]
+            c = np.where(c < 0, -c, c)
+            c = np.where(c > lim, 2 * lim - c, c)
+            pos[:, k] = np.clip(c, 0, lim)
+    return out
+
+
+def make_movie_device(spec, device="cuda", chunk=16):
+    """Render ``spec`` on the device (libgt gt_synth_render: Philox4x32-10
+    noise, the make_movie spot model).  Returns a (T, H, W) int16 CUDA
+    tensor holding the u16 pixels."""
+    import ctypes
+
+    import torch
+
+    from . import _native
+
+    tracks = torch.from_numpy(spot_tracks(spec)).to(device)
+    T, H, W = spec.frames, spec.height, spec.width
+    out = torch.empty((T, H, W), dtype=torch.int16, device=device)
+    scratch = torch.empty((min(chunk, T), H, W), dtype=torch.float32, device=device)
+    rc = _native.load().gt_synth_render(ctypes.c_void_p(tracks.data_ptr()), spec.spots, T, H, W, spec.sigma,
+                                        spec.background, spec.read_noise, spec.seed, ctypes.c_void_p(out.data_ptr()),
+                                        ctypes.c_void_p(scratch.data_ptr()), min(chunk, T),
+                                        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    if rc != 0:
+        raise RuntimeError(f"gt_synth_render failed ({rc})")
+    torch.cuda.current_stream().synchronize()
+    return out
