@@ -55,6 +55,24 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(x, world, device):
+    """The largest x over all ranks (every rank gets it); x itself at N=1."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank, world, ms_max):
+    """Whole-job units/s: every rank processed units_per_rank, the job took
+    the slowest rank's time (replicas, weak scaling)."""
+    return world * units_per_rank / (ms_max / 1e3)
+
+
 def locate_traffic(frames):
     """DRAM bytes (read + write) of one locate launch over `frames` frames:
     the per-frame figure of the committed ncu capture of the same kernel on
@@ -481,11 +499,8 @@ def main():
     if world > 1:
         dist.barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
-    t = torch.tensor([ms], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * T / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, world, f"cuda:{local}")
+    value = aggregate_rate(T, world, ms_max)
 
     # end to end through the public API: pinned host frames in, table out
     e2e_value, tab, pinned = None, None, None
@@ -501,10 +516,7 @@ def main():
         for _ in range(e2e_steps):
             tab, cols = batch_rust(host_in, **params)
         e2e_s = (time.perf_counter() - t0) / e2e_steps
-        te = torch.tensor([e2e_s], device=f"cuda:{local}")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_value = world * T / float(te.item())
+        e2e_value = aggregate_rate(T, world, max_over_ranks(e2e_s, world, f"cuda:{local}") * 1e3)
 
     if rank == 0:
         loc_ms = float(np.median([s["ms_locate"] for s in stats]))
