@@ -525,14 +525,32 @@ struct Linker {
         const size_t NS = prev.size(), ND = dest.size();
         std::vector<std::vector<size_t>> s2d(NS);
         std::vector<std::vector<std::pair<size_t, float>>> d2s(ND);
-        for (size_t s = 0; s < NS; ++s)
-            for (size_t d = 0; d < ND; ++d) {
-                float dd;
-                if (within(prev[s].y, prev[s].x, dest[d][0], dest[d][1], radius, &dd)) {
-                    s2d[s].push_back(d);
-                    d2s[d].push_back({s, dd});
+        // candidate pairs through a uniform grid of cell size `radius` over
+        // the destinations (+-2 cells, so that no pair passing `within` is
+        // missed to rounding); each source's list is then put in ascending
+        // destination order, exactly the order of an all-pairs scan
+        std::unordered_map<long long, std::vector<size_t>> grid;
+        auto cell = [&](float v) { return (long long)std::floor(v / radius); };
+        auto key = [](long long a, long long b) { return a * 1000003LL + b; };
+        for (size_t d = 0; d < ND; ++d) grid[key(cell(dest[d][0]), cell(dest[d][1]))].push_back(d);
+        for (size_t s = 0; s < NS; ++s) {
+            const long long cy = cell(prev[s].y), cx = cell(prev[s].x);
+            for (long long a = cy - 2; a <= cy + 2; ++a)
+                for (long long b = cx - 2; b <= cx + 2; ++b) {
+                    auto it = grid.find(key(a, b));
+                    if (it == grid.end()) continue;
+                    for (size_t d : it->second) {
+                        float dd;
+                        if (within(prev[s].y, prev[s].x, dest[d][0], dest[d][1], radius, &dd)) s2d[s].push_back(d);
+                    }
                 }
+            std::sort(s2d[s].begin(), s2d[s].end());
+            for (size_t d : s2d[s]) {
+                float dd = 0.0f;
+                within(prev[s].y, prev[s].x, dest[d][0], dest[d][1], radius, &dd);
+                d2s[d].push_back({s, dd});
             }
+        }
         std::vector<char> vis_s(NS, 0), vis_d(ND, 0);
         std::vector<int64_t> output(ND, -2);  // -2 = None (unassigned)
         std::vector<std::pair<std::vector<size_t>, std::vector<size_t>>> paths;

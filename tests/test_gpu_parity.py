@@ -6,6 +6,8 @@ compared for exact equality, because the kernels evaluate every value with
 the oracle's operation order (explicit fused multiply-adds only).  Each case
 also states the error of the FP32 result against the FP64 oracle.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -191,22 +193,30 @@ def test_locate_kernel_variants_agree(gpu, opt):
 
 
 def test_full_size_plain_1000(gpu):
-    """All 1000 frames of 512^2 on the GPU; locate of sampled frames and the
-    whole linking checked against the oracle."""
+    """All 1000 frames of 512^2 (the throughput workload) on the GPU against
+    the oracle over the whole movie: every row, column and trajectory id."""
     spec = synth.PLAIN_1000
     mv = synth.make_movie(spec)
     params = dict(spec.params, cpu_processed=True)
-    tab, cols = batch_rust(mv, **params)
-    assert tab.shape[0] > 1000 * 300
-    frames = np.unique(tab[:, 0]).astype(int)
-    assert len(frames) == 1000
-    # locate: frames are independent
-    for t in [0, 1, 377, 998, 999]:
-        want, _ = oracle.batch(mv[t:t + 1], nthreads=1, **dict(params, search_range=None, memory=None))
-        got = tab[tab[:, 0] == t][:, [0, 1, 2, 3, 5, 6, 7]].copy()
-        got[:, 0] = 0
-        np.testing.assert_array_equal(got, want)
-    # linking of the whole movie (size-independent property: the sequential
-    # linker on the GPU's own table gives the same trajectory IDs)
-    ids = oracle.link(tab[:, :4], spec.params["search_range"], spec.params["memory"])
-    np.testing.assert_array_equal(tab[:, 4].astype(np.uint64), ids)
+    got = batch_rust(mv, **params)
+    assert got[0].shape[0] > 1000 * 300
+    d = params.pop("diameter")
+    want = oracle.batch(mv, d, nthreads=os.cpu_count() or NTHREADS, **params)
+    assert_tables_equal(got, want, None)
+
+
+def test_full_size_dense_linking(gpu):
+    """The dense linking stress at full size: 200 frames of 2048^2 with 20000
+    spots, step 2.5 px, search_range 7, memory 3, diameter 9 -- every row and
+    trajectory id against the oracle."""
+    spec = synth.DENSE_LINK
+    mv = synth.make_movie_device(spec).cpu().numpy().view(np.uint16)  # 838 Mpx: rendered on the device
+    params = dict(spec.params)
+    got = batch_rust(mv, **params)
+    st = _native.last_stats()
+    assert got[0].shape[0] > 200 * 12000
+    d = params.pop("diameter")
+    want = oracle.batch(mv, d, nthreads=os.cpu_count() or NTHREADS, **params)
+    assert_tables_equal(got, want, None)
+    print(f"dense linking: {got[0].shape[0]} rows, {int(got[0][:, 4].max()) + 1} trajectories, "
+          f"link passes {st['link_iterations']}, link {st['ms_link']:.2f} ms")

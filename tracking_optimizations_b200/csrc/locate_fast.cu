@@ -325,6 +325,9 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
             if (!done) {
                 atomicOr(b.err, ERR_DEVICE_TIMEOUT);
                 s_fail = 1;
+                // give the copy in flight a second bounded wait to land in
+                // this CTA's shared memory before the CTA exits
+                for (int it = 0; it < (1 << 22) && !done; ++it) done = mbar_try_wait(&bar, 0);
             }
         }
         __syncthreads();

@@ -84,7 +84,8 @@ def make_movie(spec, return_truth=False):
         val = a[:, None, None] * np.exp(-((rows - p[:, 0, None, None]) ** 2 +
                                           (cols - p[:, 1, None, None]) ** 2) * inv2s2)
         ok = (rows >= 0) & (rows < H) & (cols >= 0) & (cols < W)
-        np.add.at(img, (rows[ok], cols[ok]), val[ok])
+        img += np.bincount((rows[ok] * W + cols[ok]).ravel(), weights=val[ok].ravel(),
+                           minlength=H * W).reshape(H, W)
         movie[t] = np.clip(np.rint(img), 0, 65535).astype(np.uint16)
         pos = pos + rng.normal(0.0, spec.step, (N, 2))
         # reflect at the borders
