@@ -71,6 +71,8 @@ struct gt_ctx {
     size_t h_status_n = 0;
     int tune_disabled = 0;
     int batch_cap_div = 64;           // first candidate capacity of batched movies: H*W / this
+    cudaStream_t copy_stream = nullptr;  // host->device frame chunks
+    cudaEvent_t cev[9] = {};
 };
 
 namespace {
@@ -80,6 +82,10 @@ constexpr int LOC_TW = 64;
 constexpr int LOC_CMAX = 512;
 constexpr int FB_WIN_MAX = 100;
 constexpr long long SUBNET_BUDGET = 1LL << 26;  // option trials per subnet
+// shared-memory pool of a linker block: 4 blocks of 256 threads per SM, so
+// that one round of blocks covers ~600 frames; frames whose data does not
+// fit use the block's global scratch slot
+constexpr int LINK_POOL_BYTES = 48 * 1024;
 
 struct Resolved {
     // lib.rs:77-91 defaults
@@ -477,7 +483,7 @@ int run_link(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
     int rounds = 1;
     while ((1 << rounds) < T + 1) ++rounds;
     rounds += 1;
-    L.lsm_bytes = 96 * 1024;
+    L.lsm_bytes = LINK_POOL_BYTES;
     CK(cudaFuncSetAttribute(link_fixpoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.lsm_bytes));
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_kernel, 256, L.lsm_bytes));
@@ -557,8 +563,13 @@ int fast_division(gt_ctx* ctx, const Plan& P, FixedDiv* dn, FixedDiv* dk, bool* 
 }
 
 // The whole locate(+link) pipeline on device frames; table left in w.out.
+// With h_frames set, d_frames is the workspace copy of host frames: the
+// copy runs in chunks of frames on the context's copy stream and each
+// chunk's locate launch waits only for its own chunk, so host->device
+// transfer and locate overlap.
 int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames, cudaStream_t st,
-                 int* err_bits, int64_t* nrows, int* d_walk = nullptr, int64_t walk_rows = 0) {
+                 int* err_bits, int64_t* nrows, int* d_walk = nullptr, int64_t walk_rows = 0,
+                 const void* h_frames = nullptr, size_t elem = 0) {
     const int T = P.T;
     MovieBufs b = movie_bufs(P, w, d_frames);
     int rc = upload_tables(ctx, P, w, st);
@@ -579,10 +590,33 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
         fast = ok;  // otherwise the generic kernel (IEEE division)
     }
     ctx->stats.locate_kernel = fast ? 1 : 0;
+    // frame chunks: up to 8 for host frames (copy/locate overlap), else
+    // as large as the grid allows
+    const int chunk = h_frames ? std::min(65535, std::max(16, (T + 7) / 8)) : 65535;
+    const size_t fbytes = (size_t)P.H * P.W * elem;
+    int ci = 0;
+    auto stage = [&](int f0, int nf) -> int {
+        if (!h_frames) return GT_OK;
+        if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        for (auto& e : ctx->cev)
+            if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        if (ci == 0) {
+            CK(cudaEventRecord(ctx->cev[8], st));
+            CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->cev[8], 0));
+        }
+        CK(cudaMemcpyAsync((char*)d_frames + (size_t)f0 * fbytes, (const char*)h_frames + (size_t)f0 * fbytes,
+                           (size_t)nf * fbytes, cudaMemcpyHostToDevice, ctx->copy_stream));
+        CK(cudaEventRecord(ctx->cev[ci & 7], ctx->copy_stream));
+        CK(cudaStreamWaitEvent(st, ctx->cev[ci & 7], 0));
+        ++ci;
+        return GT_OK;
+    };
     if (fast) {
         CK(cudaEventRecord(ctx->ev[0], st));
-        for (int f0 = 0; f0 < T; f0 += 65535) {
-            dim3 grid(ntiles, std::min(65535, T - f0));
+        for (int f0 = 0; f0 < T; f0 += chunk) {
+            rc = stage(f0, std::min(chunk, T - f0));
+            if (rc) return rc;
+            dim3 grid(ntiles, std::min(chunk, T - f0));
             int used_tma = 0;
             CK(launch_locate_fast(P.lp.krad, P.lp.D, P.lp.rint_c, P.fast_th, grid, st, P.lp, b, dn, dk, T, f0,
                                   &used_tma));
@@ -596,8 +630,10 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
         lg.ntx = (P.W + LOC_TW - 1) / LOC_TW;
         lg.nty = (P.H + LOC_TH - 1) / LOC_TH;
         CK(cudaEventRecord(ctx->ev[0], st));
-        for (int f0 = 0; f0 < T; f0 += 65535) {
-            dim3 grid(lg.ntx * lg.nty, std::min(65535, T - f0));
+        for (int f0 = 0; f0 < T; f0 += chunk) {
+            rc = stage(f0, std::min(chunk, T - f0));
+            if (rc) return rc;
+            dim3 grid(lg.ntx * lg.nty, std::min(chunk, T - f0));
             locate_tiles_kernel<<<grid, 256, P.smem_loc, st>>>(lg, b, f0);
             ctx->stats.launches += 1;
         }
@@ -717,14 +753,11 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
         rc = ensure_arena(ctx, need);
         if (rc) return rc;
         carve(P, ctx->arena, &w, fbytes, true);
-        const void* dfr = frames;
-        if (host) {
-            CK(cudaMemcpyAsync(w.frames, frames, fbytes, cudaMemcpyHostToDevice, st));
-            dfr = w.frames;
-        }
+        const void* dfr = host ? w.frames : frames;
         int bits = 0;
         int64_t nrows = 0;
-        rc = run_pipeline(ctx, P, w, dfr, st, &bits, &nrows, d_walk, d_walk ? out_rows : 0);
+        rc = run_pipeline(ctx, P, w, dfr, st, &bits, &nrows, d_walk, d_walk ? out_rows : 0, host ? frames : nullptr,
+                          elem_size(dtype));
         if (rc) return rc;
         bool retry;
         rc = err_status(ctx, bits, &retry);
@@ -940,7 +973,7 @@ int enqueue_batch(gt_ctx* ctx, std::vector<BatchMovie>& B, gt_movie* mv, int n, 
         int* ps = S.d_passes;
         void* args[] = {(void*)&Ls, (void*)&mem, (void*)&fst, &nm, &mp, &nd, &ps};
         CK(cudaLaunchCooperativeKernel((const void*)link_fixpoint_multi_kernel, dim3(S.link_grid), dim3(256), args,
-                                       96 * 1024, st));
+                                       LINK_POOL_BYTES, st));
         S.launches += 1;
     }
     CK(cudaEventRecord(ctx->bev[9], st));
@@ -1032,9 +1065,9 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         S.max_passes = std::max(S.max_passes, P.T + 1);
     }
     if (S.nlink > 0) {
-        CK(cudaFuncSetAttribute(link_fixpoint_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        CK(cudaFuncSetAttribute(link_fixpoint_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, LINK_POOL_BYTES));
         int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_multi_kernel, 256, 96 * 1024));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_multi_kernel, 256, LINK_POOL_BYTES));
         const size_t per_slot = 4 * (3 * st_s + st_s1) + 8 * st_e * 2 + 4 * st_p1 + 4 * 4 * st_n + st_n + 16 * st_n +
                                 4 + 8 * st_h;
         const size_t budget = (size_t)6 << 30;
@@ -1123,7 +1156,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
             L.uf = pool.uf; L.c_nd = pool.c_nd; L.c_ns = pool.c_ns; L.c_min = pool.c_min; L.vis = pool.vis;
             L.work = pool.work; L.bump = pool.bump; L.hkey = pool.hkey; L.hval = pool.hval;
             L.st_s = st_s; L.st_s1 = st_s1; L.st_p1 = st_p1; L.st_n = st_n; L.st_e = st_e; L.st_h = st_h;
-            L.lsm_bytes = 96 * 1024;
+            L.lsm_bytes = LINK_POOL_BYTES;
             hL[B[i].link_slot] = L;
             hm[B[i].link_slot] = (int)B[i].P.r.memory;
             hf[B[i].link_slot] = fs;
@@ -1375,6 +1408,9 @@ void gt_ctx_destroy(gt_ctx* ctx) {
     if (ctx->arena) cudaFree(ctx->arena);
     if (ctx->d_count) cudaFree(ctx->d_count);
     if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    for (auto& e : ctx->cev)
+        if (e) cudaEventDestroy(e);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     for (auto& sd : ctx->side)
         if (sd) cudaStreamDestroy(sd);

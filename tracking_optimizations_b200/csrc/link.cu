@@ -166,8 +166,11 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
             const int nnode = ns + nd;
             // the frame's particles, grid and scratch live in shared memory
             // when they fit (latency), else in this block's global slot
-            const int need = 3 * nd + ncell + 1 + 4 * ns + 1 + nd + 1 + 8 * nnode + (nnode + 3) / 4;
-            const bool sm = need <= pool;
+            // the cell index is staged too when it fits beside the rest
+            const int need_rest = 3 * nd + 4 * ns + 1 + nd + 1 + 8 * nnode + (nnode + 3) / 4;
+            const bool sm = need_rest <= pool;
+            const bool grid_sm = sm && need_rest + ncell + 1 <= pool;
+            const int need = need_rest + (grid_sm ? ncell + 1 : 0);
             int* o = lsm;
             auto take = [&](int n) { int* q = o; o += n; return q; };
             const float* dy;
@@ -180,15 +183,20 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
             if (sm) {
                 float* ddy = (float*)take(nd);
                 float* ddx = (float*)take(nd);
-                int* ggs = take(ncell + 1);
                 int* ggi = take(nd);
                 const float* py_t = L.py + (size_t)t * cap_p;
                 const float* px_t = L.px + (size_t)t * cap_p;
                 const int* gs_t = L.gstart + (size_t)t * (ncell + 1);
                 const int* gi_t = L.gidx + (size_t)t * cap_p;
                 for (int i = threadIdx.x; i < nd; i += NTL) { ddy[i] = py_t[i]; ddx[i] = px_t[i]; ggi[i] = gi_t[i]; }
-                for (int i = threadIdx.x; i <= ncell; i += NTL) ggs[i] = gs_t[i];
-                dy = ddy; dx = ddx; gs = ggs; gi = ggi;
+                if (grid_sm) {
+                    int* ggs = take(ncell + 1);
+                    for (int i = threadIdx.x; i <= ncell; i += NTL) ggs[i] = gs_t[i];
+                    gs = ggs;
+                } else {
+                    gs = gs_t;
+                }
+                dy = ddy; dx = ddx; gi = ggi;
                 sy = (float*)take(ns); sx = (float*)take(ns); sh = take(ns); sdeg = take(ns + 1);
                 dcnt = take(nd + 1);
                 uf = take(nnode); cnd = take(nnode); cns = take(nnode); cmin = take(nnode);

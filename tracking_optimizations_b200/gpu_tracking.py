@@ -13,6 +13,7 @@ accepted as well.  Unsupported options raise NotImplementedError as the
 reference's `not_implemented!` does (lib.rs:28-39, 73-74).
 """
 import ctypes
+import weakref
 
 import numpy as np
 
@@ -61,11 +62,22 @@ def batch_rust(pyarr, diameter, minmass=None, maxsize=None, separation=None, noi
     _native.check(st, ctx)
     try:
         n, c = tab.nrows, tab.ncols
-        out = np.ctypeslib.as_array(tab.data, shape=(max(n, 1) * c,))[: n * c].copy().reshape(n, c)
         cols = [(tab.names[i].value.decode(), tab.types[i].value.decode()) for i in range(c)]
-    finally:
+        out = _adopt_table(lib, tab, n, c)
+    except BaseException:
         lib.gt_table_free(ctypes.byref(tab))
+        raise
     return out, cols
+
+
+def _adopt_table(lib, tab, n, c):
+    """The (n, c) float32 table that libgt allocated, as a numpy array that
+    owns it: no copy; gt_table_free runs when the array is collected."""
+    buf = (ctypes.c_float * max(n * c, 1)).from_address(ctypes.addressof(tab.data.contents))
+    keep = _native.GtTable()
+    ctypes.pointer(keep)[0] = tab
+    weakref.finalize(buf, lib.gt_table_free, ctypes.byref(keep))
+    return np.frombuffer(buf, dtype=np.float32, count=n * c).reshape(n, c)
 
 
 def batch_device(frames, diameter, **params):
