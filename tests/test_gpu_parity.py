@@ -175,7 +175,7 @@ def test_link_rust_matches_oracle(gpu):
     np.testing.assert_array_equal(link_rust(quirky, 6.0, 2), oracle.link(quirky, 6.0, 2))
 
 
-@pytest.mark.parametrize("opt", [("locate_tile_rows", 64), ("force_generic", 1)])
+@pytest.mark.parametrize("opt", [("locate_tile_rows", 32), ("force_generic", 1)])
 def test_locate_kernel_variants_agree(gpu, opt):
     """The specialised kernel at both tile heights and the generic kernel
     produce identical tables."""
@@ -187,7 +187,7 @@ def test_locate_kernel_variants_agree(gpu, opt):
         _native.set_option(*opt)
         other = batch_rust(mv, **params)
     finally:
-        _native.set_option("locate_tile_rows", 32)
+        _native.set_option("locate_tile_rows", 64)
         _native.set_option("force_generic", 0)
     assert_tables_equal(other, base, None)
 

@@ -89,25 +89,18 @@ __device__ __forceinline__ int box_count(int pp, int q, int n, int kr) {
     return (abs(q - pp) <= kr) + (abs(-q - 1 - pp) <= kr) + (abs(2 * n - q - 1 - pp) <= kr);
 }
 
-template <int NT>
-__device__ __forceinline__ float block_sum(float v, float* red) {
+__device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) red[wid] = v;
-    __syncthreads();
-    float s = 0.f;
-    if (threadIdx.x == 0)
-        for (int q = 0; q < NT / 32; ++q) s += red[q];
-    return s;  // valid in thread 0
+    return v;  // every lane
 }
 
 }  // namespace
 
 enum AdjMode { ADJ_FORWARD = 0, ADJ_BACKWARD = 1, ADJ_UNCERTAINTY = 2 };
 
-// One CTA per particle (grid-stride).  walk rows: {frame, ul, vl, up, vp}.
+// One warp per particle (grid-stride over warps), ADJ_NT / 32 warps per
+// CTA sharing the circle table.  walk rows: {frame, ul, vl, up, vp}.
 // FORWARD writes yxm (n x 3).  BACKWARD reads grad (n x 3), adds dL/dR into
 // the zeroed plane gR (T x H x W) and dL/d{noise_size, smoothing_size} into
 // gpar.  UNCERTAINTY writes the standard deviations of (y, x, mass) under
@@ -119,30 +112,32 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
                                                                   const float* __restrict__ grad, float* yxm,
                                                                   float* gR, double* gpar, int* err) {
     extern __shared__ __align__(16) float asm_[];
+    constexpr int NW = ADJ_NT / 32;
     const int K = p.K;
-    int* sci = (int*)asm_;            // 2K circle offsets {i, j}
-    float* sR = asm_ + 2 * K;         // R at the circle pixels
-    float* sB = sR + K;               // B
-    float* sD = sB + K;               // dG/ds
-    float* sJ = sD + K;               // 3K: dy/dR, dx/dR, dm/dR (uncertainty)
-    __shared__ float red[ADJ_NT / 32];
-    __shared__ float cen[3];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int* sci = (int*)asm_;                      // 2K circle offsets {i, j}, shared
+    float* sR = asm_ + 2 * K + wid * 6 * K;     // this warp's R at the circle pixels
+    float* sB = sR + K;                         // B
+    float* sD = sB + K;                         // dG/ds
+    float* sJ = sD + K;                         // 3K: dy/dR, dx/dR, dm/dR (uncertainty)
     for (int q = threadIdx.x; q < 2 * K; q += ADJ_NT) sci[q] = circ[q];
+    __syncthreads();
     const int H = p.H, W = p.W, kr = p.krad, b = p.border;
-    for (long long k = blockIdx.x; k < n; k += gridDim.x) {
+    const long long wstride = (long long)gridDim.x * NW;
+    for (long long k = (long long)blockIdx.x * NW + wid; k < n; k += wstride) {
         const int* wr = walk + 5 * k;
         const int t = __ldg(wr), ul = __ldg(wr + 1), vl = __ldg(wr + 2), up = __ldg(wr + 3), vp = __ldg(wr + 4);
         const bool valid = t >= 0 && t < p.T && ul >= 0 && ul < H && vl >= 0 && vl < W && up >= 0 && up < H &&
                            vp >= 0 && vp < W;
         if (!valid) {
-            if (threadIdx.x == 0) atomicOr(err, 1);
+            if (lane == 0) atomicOr(err, 1);
             continue;
         }
         const bool interior = !(ul - b < 0 || ul + b >= H || vl - b < 0 || vl + b >= W);
         if (!interior) {
             // centers.wgsl border band: offset (0, 0), mass 0, no dependence
             // on the frame
-            if (threadIdx.x == 0) {
+            if (lane == 0) {
                 if (MODE == ADJ_FORWARD) {
                     yxm[3 * k] = (float)up; yxm[3 * k + 1] = (float)vp; yxm[3 * k + 2] = 0.f;
                 } else if (MODE == ADJ_UNCERTAINTY) {
@@ -152,15 +147,16 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
             continue;
         }
         const float* fr = frames + (size_t)t * H * W;
-        __syncthreads();  // smem of the previous particle is free
-        for (int c = threadIdx.x; c < K; c += ADJ_NT) {
+        __syncwarp();  // the previous particle's reads of this warp's arrays are done
+        for (int c = lane; c < K; c += 32) {
             const BpTerms bt = bandpass_terms(p, fr, ul + sci[2 * c], vl + sci[2 * c + 1]);
             sR[c] = bt.r;
             sB[c] = bt.bmean;
             sD[c] = bt.dg;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        __syncwarp();
+        float c0 = 0.f, c1 = 0.f, m = 0.f;
+        if (lane == 0) {
             // centers.wgsl:23-109 accumulation order (i outer, j inner)
             float a0 = 0.f, a1 = 0.f, mm = 0.f;
             for (int c = 0; c < K; ++c) {
@@ -169,14 +165,15 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
                 a1 = fmaf(data, (float)sci[2 * c + 1], a1);
                 mm = mm + data;
             }
-            cen[0] = a0 / mm;
-            cen[1] = a1 / mm;
-            cen[2] = mm;
+            c0 = a0 / mm;
+            c1 = a1 / mm;
+            m = mm;
         }
-        __syncthreads();
-        const float c0 = cen[0], c1 = cen[1], m = cen[2];
+        c0 = __shfl_sync(0xffffffffu, c0, 0);
+        c1 = __shfl_sync(0xffffffffu, c1, 0);
+        m = __shfl_sync(0xffffffffu, m, 0);
         if constexpr (MODE == ADJ_FORWARD) {
-            if (threadIdx.x == 0) {
+            if (lane == 0) {
                 yxm[3 * k] = (float)up + c0;
                 yxm[3 * k + 1] = (float)vp + c1;
                 yxm[3 * k + 2] = m;
@@ -186,7 +183,7 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
         if (!(m > 0.f) || !isfinite(m)) {
             // zero mass: the centroid is undefined and the row is never
             // emitted (mass > minmass and mass != 0)
-            if (MODE == ADJ_UNCERTAINTY && threadIdx.x == 0) {
+            if (MODE == ADJ_UNCERTAINTY && lane == 0) {
                 yxm[3 * k] = 0.f; yxm[3 * k + 1] = 0.f; yxm[3 * k + 2] = 0.f;
             }
             continue;
@@ -196,7 +193,7 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
             const float gy = __ldg(grad + 3 * k), gx = __ldg(grad + 3 * k + 1), gm = __ldg(grad + 3 * k + 2);
             float ds = 0.f, dk = 0.f;
             float* plane = gR + (size_t)t * H * W;
-            for (int c = threadIdx.x; c < K; c += ADJ_NT) {
+            for (int c = lane; c < K; c += 32) {
                 if (!(sR[c] > 0.f)) continue;
                 const float ic = (float)sci[2 * c], jc = (float)sci[2 * c + 1];
                 const float g = gm + (gy * (ic - c0) + gx * (jc - c1)) * inv_m;
@@ -204,27 +201,26 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
                 ds = fmaf(g, sD[c], ds);
                 dk = fmaf(g, 2.f * sB[c] / p.k, dk);
             }
-            const float tds = block_sum<ADJ_NT>(ds, red);
-            const float tdk = block_sum<ADJ_NT>(dk, red);
-            if (threadIdx.x == 0) {
+            const float tds = warp_sum(ds), tdk = warp_sum(dk);
+            if (lane == 0) {
                 atomicAdd(gpar, (double)tds);
                 atomicAdd(gpar + 1, (double)tdk);
             }
             continue;
         }
         if constexpr (MODE == ADJ_UNCERTAINTY) {
-            // UNCERTAINTY: Jacobian rows over the window that the circle's
-            // bandpass reads, J(q) = sum_c dR_c/dI(q) * dOut/dR_c
-            for (int c = threadIdx.x; c < K; c += ADJ_NT) {
+            // Jacobian rows over the window that the circle's bandpass
+            // reads, J(q) = sum_c dR_c/dI(q) * dOut/dR_c
+            for (int c = lane; c < K; c += 32) {
                 const bool on = sR[c] > 0.f;
                 sJ[c] = on ? ((float)sci[2 * c] - c0) * inv_m : 0.f;
                 sJ[K + c] = on ? ((float)sci[2 * c + 1] - c1) * inv_m : 0.f;
                 sJ[2 * K + c] = on ? 1.f : 0.f;
             }
-            __syncthreads();
+            __syncwarp();
             const int WR = p.rc + kr, WS = 2 * WR + 1;
             float vy = 0.f, vx = 0.f, vm = 0.f;
-            for (int q = threadIdx.x; q < WS * WS; q += ADJ_NT) {
+            for (int q = lane; q < WS * WS; q += 32) {
                 const int qu = ul - WR + q / WS, qv = vl - WR + q % WS;
                 if (qu < 0 || qu >= H || qv < 0 || qv >= W) continue;
                 float jy = 0.f, jx = 0.f, jm = 0.f;
@@ -245,10 +241,8 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
                 vx = fmaf(jx * jx, var, vx);
                 vm = fmaf(jm * jm, var, vm);
             }
-            const float ty = block_sum<ADJ_NT>(vy, red);
-            const float tx = block_sum<ADJ_NT>(vx, red);
-            const float tm = block_sum<ADJ_NT>(vm, red);
-            if (threadIdx.x == 0) {
+            const float ty = warp_sum(vy), tx = warp_sum(vx), tm = warp_sum(vm);
+            if (lane == 0) {
                 yxm[3 * k] = sqrtf(ty);
                 yxm[3 * k + 1] = sqrtf(tx);
                 yxm[3 * k + 2] = sqrtf(tm);
@@ -280,12 +274,21 @@ __global__ void __launch_bounds__(TR_NT) adjoint_transpose_kernel(AdjParams p, c
         S[q] = (gu >= 0 && gu < H && gv >= 0 && gv < W) ? __ldg(src + (size_t)gu * W + gv) : 0.f;
     }
     __syncthreads();
+    // away from the left/right frame edges every box tap counts once
+    const bool cols_inner = v0 >= kr && v0 + TR_TW <= W - kr;
+    const bool rows_inner = u0 >= kr && u0 + TR_TH <= H - kr;
     for (int q = threadIdx.x; q < SH * TR_TW; q += TR_NT) {
         const int r = q / TR_TW, c = q % TR_TW;
         const int qv = v0 + c;
         float g = 0.f, bx = 0.f;
-        if (qv < W) {
-            const float* srow = S + r * SW + c + kr;
+        const float* srow = S + r * SW + c + kr;
+        if (cols_inner) {
+            for (int j = -kr; j <= kr; ++j) {
+                const float s = srow[j];
+                g = fmaf(p.a[j + kr], s, g);
+                bx = bx + s;
+            }
+        } else if (qv < W) {
             for (int j = -kr; j <= kr; ++j) {
                 const float s = srow[j];
                 g = fmaf(p.a[j + kr], s, g);
@@ -303,17 +306,25 @@ __global__ void __launch_bounds__(TR_NT) adjoint_transpose_kernel(AdjParams p, c
         const int qu = u0 + r, qv = v0 + c;
         if (qu >= H || qv >= W) continue;
         float g = 0.f, bx = 0.f;
-        for (int i = -kr; i <= kr; ++i) {
-            const int rr = (r + kr + i) * TR_TW + c;
-            g = fmaf(p.a[i + kr], RG[rr], g);
-            const int pu = qu + i;
-            if (pu >= 0 && pu < H) bx = fmaf((float)box_count(pu, qu, H, kr), RB[rr], bx);
+        if (rows_inner) {
+            for (int i = -kr; i <= kr; ++i) {
+                const int rr = (r + kr + i) * TR_TW + c;
+                g = fmaf(p.a[i + kr], RG[rr], g);
+                bx = bx + RB[rr];
+            }
+        } else {
+            for (int i = -kr; i <= kr; ++i) {
+                const int rr = (r + kr + i) * TR_TW + c;
+                g = fmaf(p.a[i + kr], RG[rr], g);
+                const int pu = qu + i;
+                if (pu >= 0 && pu < H) bx = fmaf((float)box_count(pu, qu, H, kr), RB[rr], bx);
+            }
         }
         dst[(size_t)qu * W + qv] = g - bx / p.kk;
     }
 }
 
-size_t adjoint_particle_smem(int K) { return sizeof(float) * (size_t)(2 * K + 3 * K + 3 * K); }
+size_t adjoint_particle_smem(int K) { return sizeof(float) * (size_t)(2 * K + (ADJ_NT / 32) * 6 * K); }
 
 size_t adjoint_transpose_smem(int kr) {
     const int SH = TR_TH + 2 * kr, SW = TR_TW + 2 * kr;
@@ -325,7 +336,7 @@ cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* 
                                      int* err, int num_sms, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const size_t smem = adjoint_particle_smem(p.K);
-    const int grid = (int)std::min<long long>(n, (long long)num_sms * 16);
+    const int grid = (int)std::min<long long>((n + ADJ_NT / 32 - 1) / (ADJ_NT / 32), (long long)num_sms * 16);
     cudaError_t e = cudaSuccess;
     switch (mode) {
         case ADJ_FORWARD:

@@ -60,7 +60,7 @@ struct gt_ctx {
     std::map<uint32_t, bool> div_ok;  // divisor bits -> fast division verified exact
     unsigned int* d_count = nullptr;
     int force_generic = 0;            // always use locate_tiles_kernel
-    int fast_tile_rows = 32;          // output tile height of the fast kernel (32 or 64)
+    int fast_tile_rows = 64;          // output tile height of the fast kernel (32 or 64)
     // batched path (gt_batch_many_device)
     std::map<std::array<int, 6>, int> tile_rows;  // autotuned tile rows per (H, W, krad, D, rc, dtype)
     std::string batch_key;            // inputs of the cached graph
@@ -833,7 +833,7 @@ int tune_tile_rows(gt_ctx* ctx, BatchMovie& bm, const void* frames, cudaStream_t
     Plan& P = bm.P;
     const std::array<int, 6> key{P.H, P.W, P.lp.krad, P.lp.D, P.lp.rint_c, P.dtype};
     auto it = ctx->tile_rows.find(key);
-    int best = 32;
+    int best = P.fast_th;
     if (it != ctx->tile_rows.end()) {
         best = it->second;
     } else if (!ctx->tune_disabled) {
@@ -1015,7 +1015,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         std::string msg;
         int rc = resolve(&m.params, &r, &msg);
         if (rc) { ctx->err = who + msg; return rc; }
-        rc = make_plan(r, m.T, m.H, m.W, m.dtype, 1, ctx->num_sms, &B[i].P, &msg, ctx->force_generic, 32,
+        rc = make_plan(r, m.T, m.H, m.W, m.dtype, 1, ctx->num_sms, &B[i].P, &msg, ctx->force_generic, ctx->fast_tile_rows,
                        ctx->batch_cap_div);
         if (rc) { ctx->err = who + msg; return rc; }
         char buf[128];

@@ -35,7 +35,11 @@ namespace gt {
 
 namespace {
 constexpr int FT = 64;    // output tile width
-constexpr int FNT = 256;  // threads
+constexpr int FNT = 256;  // threads of a 32-row tile
+
+// 8 warps per 32 output rows: 64-row tiles (less halo recomputed per
+// output row) keep 16 warps per SM slot at 2 CTAs per SM
+__host__ __device__ constexpr int fast_threads(int th) { return th == 32 ? FNT : 2 * FNT; }
 constexpr int FM = 8;     // outputs per thread item
 constexpr int FCMAX = 512;
 
@@ -270,16 +274,17 @@ __device__ __forceinline__ bool centroid_fixed(const LocParams& p, const P2Acc<G
 }  // namespace
 
 template <int KR, int DD, int TH0, int RC>
-__global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
+__global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     locate_fast_kernel(const LocParams p, const MovieBufs b, const FixedDiv dnorm, const FixedDiv dkk,
                        const __grid_constant__ CUtensorMap tmap, int use_tma, int frame0) {
     using G = Geo<KR, DD, TH0, RC>;
+    constexpr int NTK = fast_threads(TH0);
     constexpr int TAPS = 2 * KR + 1;
     constexpr int O = G::O;
     constexpr int HP = G::HP, HX = G::HX;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int warp_tot[FNT / 32];
+    __shared__ int warp_tot[NTK / 32];
     __shared__ int s_total, s_base, s_fail;
     __shared__ int rowcount[TH0];
     __shared__ int rowstart[TH0];
@@ -334,7 +339,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
         if (s_fail) return;
     } else {
         const unsigned short* fr = (const unsigned short*)b.frames + (size_t)t * H * W;
-        for (int i = tid; i < G::RH * G::RW; i += FNT) {
+        for (int i = tid; i < G::RH * G::RW; i += NTK) {
             const int r = i / G::RW, c = i - r * G::RW;
             const int gy = ry0 + r, gx = rx0 + c;
             unsigned short v = 0;
@@ -348,11 +353,11 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
         rowcount[tid] = 0;
     }
     if (p.cpu_processed)
-        for (int k = tid; k < G::K; k += FNT)
+        for (int k = tid; k < G::K; k += NTK)
             sc[k] = make_float2(__ldg(b.char_tab + 3 * k + 1), __ldg(b.char_tab + 3 * k + 2));
 
     // ---- 1. u16 -> f32 row pairs ----
-    for (int i = tid; i < G::RP * G::RW; i += FNT) {
+    for (int i = tid; i < G::RP * G::RW; i += NTK) {
         const int pr = i / G::RW, c = i - pr * G::RW;
         Rp[pr * G::RPS + c] = make_float2((float)U[(2 * pr) * G::RW + c], (float)U[(2 * pr + 1) * G::RW + c]);
     }
@@ -363,7 +368,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     for (int j = 0; j < TAPS; ++j) W2[j] = make_float2(p.w[j], p.w[j]);
 
     // ---- 2. row pass (preprocess_rows.wgsl) on row pairs ----
-    for (int it = tid; it < G::RP * G::NPW; it += FNT) {
+    for (int it = tid; it < G::RP * G::NPW; it += NTK) {
         const int q = it / G::RP, pr = it - q * G::RP;
         const int pc0 = q * FM;
         const float2* src = Rp + pr * G::RPS + pc0;
@@ -409,7 +414,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
 
     // ---- 3. column pass (preprocess_cols.wgsl) -> P2 ----
     const float NEG = -CUDART_INF_F;
-    for (int it = tid; it < G::PWC * G::NRQ; it += FNT) {
+    for (int it = tid; it < G::PWC * G::NRQ; it += NTK) {
         const int rq = it / G::PWC, c = it - rq * G::PWC;
         const int p0 = rq * (FM / 2);
         float2 L[FM / 2 + KR], ML[FM / 2 + KR - 1];
@@ -477,7 +482,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     __syncthreads();
 
     // ---- 4. row max over the dilation window (max_rows.wgsl) ----
-    for (int it = tid; it < G::PP * (FT / FM); it += FNT) {
+    for (int it = tid; it < G::PP * (FT / FM); it += NTK) {
         const int q = it / G::PP, pr = it - q * G::PP;
         const int tc0 = q * FM;
         const float2* src = P2 + pr * G::P2S + tc0 + HX - O;
@@ -497,7 +502,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     __syncthreads();
 
     // ---- 5. column max vs centre: non-strict local max (walk_cols.wgsl:19-36) ----
-    for (int it = tid; it < FT * (TH0 / FM); it += FNT) {
+    for (int it = tid; it < FT * (TH0 / FM); it += NTK) {
         const int tc = it % FT, rq = it / FT;
         const int tr0 = rq * FM;
         const int k0 = (tr0 + HP - O) >> 1;  // HP - O is even
@@ -528,7 +533,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     __syncthreads();
 
     // ---- 6. raster-order compaction, walks, emission ----
-    constexpr int CHUNK = TH0 * FT / FNT;  // 8 or 16 flags per thread
+    constexpr int CHUNK = TH0 * FT / NTK;  // 8 or 16 flags per thread
     const int q0 = tid * CHUNK;
     int mine = 0;
     unsigned char fl[CHUNK];
@@ -537,7 +542,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
         fl[i] = flags[q0 + i];
         mine += fl[i];
     }
-    int pos = block_excl_scan<FNT>(mine, warp_tot, &s_total);
+    int pos = block_excl_scan<NTK>(mine, warp_tot, &s_total);
     const int ncand = s_total;
 #pragma unroll
     for (int i = 0; i < CHUNK; ++i)
@@ -550,7 +555,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
     int emitted = 0;
     for (int r0 = 0; r0 < ncand; r0 += FCMAX) {
         const int nr = min(FCMAX, ncand - r0);
-        for (int c = tid; c < nr; c += FNT) {
+        for (int c = tid; c < nr; c += NTK) {
             const int q = clist[r0 + c];
             const int u0 = ty0 + q / FT, v0 = tx0 + q % FT;
             int st;
@@ -586,11 +591,11 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
             wy[c] = y; wx[c] = x; wm[c] = m; wst[c] = st; wlp[c] = lp; wfp[c] = fp;
         }
         __syncthreads();
-        const int cchunk = (nr + FNT - 1) / FNT;
+        const int cchunk = (nr + NTK - 1) / NTK;
         const int c0 = tid * cchunk, c1 = min(c0 + cchunk, nr);
         int ne = 0;
         for (int c = c0; c < c1; ++c) ne += (wst[c] != CAND_REJECT);
-        int epos = block_excl_scan<FNT>(ne, warp_tot, &s_total);
+        int epos = block_excl_scan<NTK>(ne, warp_tot, &s_total);
         const int nemit = s_total;
         if (tid == 0) {
             int base = 0;
@@ -651,7 +656,7 @@ __global__ void __launch_bounds__(FNT, (TH0 == 32 ? 4 : 2))
         emitted += nemit;
         __syncthreads();
     }
-    for (int r = tid; r < TH; r += FNT) b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = rowcount[r];
+    for (int r = tid; r < TH; r += NTK) b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = rowcount[r];
 }
 
 // Checks div1() against IEEE division for 0 and every binary32 dividend in
@@ -728,7 +733,7 @@ cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaSt
         cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD, TH, RC>,                         \
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);      \
         if (e != cudaSuccess) return e;                                                                 \
-        locate_fast_kernel<KR, DD, TH, RC><<<grid, FNT, G::SMEM, st>>>(p, b, dnorm, dkk, map, tma, frame0); \
+        locate_fast_kernel<KR, DD, TH, RC><<<grid, fast_threads(TH), G::SMEM, st>>>(p, b, dnorm, dkk, map, tma, frame0); \
         return cudaGetLastError();                                                                      \
     }
 #define GT_FAST_CASE(KR, DD, RC)                                                                        \
