@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
     __syncthreads();
     const int H = p.H, W = p.W, kr = p.krad, b = p.border;
     const long long wstride = (long long)gridDim.x * NW;
+    double acc_ds = 0.0, acc_dk = 0.0;  // this warp's parameter gradients (BACKWARD)
     for (long long k = (long long)blockIdx.x * NW + wid; k < n; k += wstride) {
         const int* wr = walk + 5 * k;
         const int t = __ldg(wr), ul = __ldg(wr + 1), vl = __ldg(wr + 2), up = __ldg(wr + 3), vp = __ldg(wr + 4);
@@ -201,11 +202,8 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
                 ds = fmaf(g, sD[c], ds);
                 dk = fmaf(g, 2.f * sB[c] / p.k, dk);
             }
-            const float tds = warp_sum(ds), tdk = warp_sum(dk);
-            if (lane == 0) {
-                atomicAdd(gpar, (double)tds);
-                atomicAdd(gpar + 1, (double)tdk);
-            }
+            acc_ds += (double)warp_sum(ds);
+            acc_dk += (double)warp_sum(dk);
             continue;
         }
         if constexpr (MODE == ADJ_UNCERTAINTY) {
@@ -249,6 +247,19 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
             }
         }
     }
+    if constexpr (MODE == ADJ_BACKWARD) {
+        // one atomic pair per block instead of one per particle (all
+        // particles add to the same two words)
+        __shared__ double red[2 * NW];
+        if (lane == 0) { red[2 * wid] = acc_ds; red[2 * wid + 1] = acc_dk; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0, c = 0.0;
+            for (int w = 0; w < NW; ++w) { a += red[2 * w]; c += red[2 * w + 1]; }
+            atomicAdd(gpar, a);
+            atomicAdd(gpar + 1, c);
+        }
+    }
 }
 
 // Transposed bandpass of dL/dR:  dL/dI = G^T gR - B^T gR.  G is separable,
@@ -256,10 +267,12 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
 // each tap by the number of reflect-padded window positions that land on it
 // (box_count), all of which lie within +-kr of the output pixel.  One CTA per
 // 32 x 64 output tile, gR staged with a kr halo (zero outside the frame).
+template <int KRT>  // smoothing half window; 0 = taken from p.krad at run time
 __global__ void __launch_bounds__(TR_NT) adjoint_transpose_kernel(AdjParams p, const float* __restrict__ gR,
                                                                   float* __restrict__ gI) {
     extern __shared__ __align__(16) float tsm[];
-    const int kr = p.krad, H = p.H, W = p.W;
+    const int kr = KRT > 0 ? KRT : p.krad;
+    const int H = p.H, W = p.W;
     const int SH = TR_TH + 2 * kr, SW = TR_TW + 2 * kr;
     float* S = tsm;               // SH x SW
     float* RG = S + SH * SW;      // SH x TR_TW, Gaussian row pass
@@ -269,58 +282,83 @@ __global__ void __launch_bounds__(TR_NT) adjoint_transpose_kernel(AdjParams p, c
     const int t = blockIdx.y;
     const float* src = gR + (size_t)t * H * W;
     for (int q = threadIdx.x; q < SH * SW; q += TR_NT) {
-        const int r = q / SW, c = q % SW;
+        const int r = q / SW, c = q - r * SW;
         const int gu = u0 - kr + r, gv = v0 - kr + c;
         S[q] = (gu >= 0 && gu < H && gv >= 0 && gv < W) ? __ldg(src + (size_t)gu * W + gv) : 0.f;
     }
     __syncthreads();
-    // away from the left/right frame edges every box tap counts once
+    // away from the frame edges every box tap counts once
     const bool cols_inner = v0 >= kr && v0 + TR_TW <= W - kr;
     const bool rows_inner = u0 >= kr && u0 + TR_TH <= H - kr;
-    for (int q = threadIdx.x; q < SH * TR_TW; q += TR_NT) {
-        const int r = q / TR_TW, c = q % TR_TW;
-        const int qv = v0 + c;
-        float g = 0.f, bx = 0.f;
-        const float* srow = S + r * SW + c + kr;
-        if (cols_inner) {
-            for (int j = -kr; j <= kr; ++j) {
-                const float s = srow[j];
-                g = fmaf(p.a[j + kr], s, g);
-                bx = bx + s;
+    if (KRT > 0 && cols_inner) {
+        constexpr int TP = 2 * KRT + 1;
+        float a[TP];
+#pragma unroll
+        for (int j = 0; j < TP; ++j) a[j] = p.a[j];
+        for (int q = threadIdx.x; q < SH * TR_TW; q += TR_NT) {
+            const int r = q / TR_TW, c = q % TR_TW;
+            const float* srow = S + r * SW + c;
+            float g = 0.f, bx = 0.f;
+#pragma unroll
+            for (int j = 0; j < TP; ++j) {
+                const float v = srow[j];
+                g = fmaf(a[j], v, g);
+                bx = bx + v;
             }
-        } else if (qv < W) {
-            for (int j = -kr; j <= kr; ++j) {
-                const float s = srow[j];
-                g = fmaf(p.a[j + kr], s, g);
-                const int pv = qv + j;
-                if (pv >= 0 && pv < W) bx = fmaf((float)box_count(pv, qv, W, kr), s, bx);
-            }
+            RG[q] = g;
+            RB[q] = bx;
         }
-        RG[q] = g;
-        RB[q] = bx;
+    } else {
+        for (int q = threadIdx.x; q < SH * TR_TW; q += TR_NT) {
+            const int r = q / TR_TW, c = q % TR_TW;
+            const int qv = v0 + c;
+            float g = 0.f, bx = 0.f;
+            const float* srow = S + r * SW + c + kr;
+            if (qv < W) {
+                for (int j = -kr; j <= kr; ++j) {
+                    const float v = srow[j];
+                    g = fmaf(p.a[j + kr], v, g);
+                    const int pv = qv + j;
+                    if (pv >= 0 && pv < W) bx = fmaf((float)box_count(pv, qv, W, kr), v, bx);
+                }
+            }
+            RG[q] = g;
+            RB[q] = bx;
+        }
     }
     __syncthreads();
     float* dst = gI + (size_t)t * H * W;
-    for (int q = threadIdx.x; q < TR_TH * TR_TW; q += TR_NT) {
-        const int r = q / TR_TW, c = q % TR_TW;
-        const int qu = u0 + r, qv = v0 + c;
-        if (qu >= H || qv >= W) continue;
-        float g = 0.f, bx = 0.f;
-        if (rows_inner) {
-            for (int i = -kr; i <= kr; ++i) {
-                const int rr = (r + kr + i) * TR_TW + c;
-                g = fmaf(p.a[i + kr], RG[rr], g);
+    const float ikk = 1.f / p.kk;
+    if (KRT > 0 && rows_inner && v0 + TR_TW <= W) {
+        constexpr int TP = 2 * KRT + 1;
+        float a[TP];
+#pragma unroll
+        for (int j = 0; j < TP; ++j) a[j] = p.a[j];
+        for (int q = threadIdx.x; q < TR_TH * TR_TW; q += TR_NT) {
+            const int r = q / TR_TW, c = q % TR_TW;
+            float g = 0.f, bx = 0.f;
+#pragma unroll
+            for (int i = 0; i < TP; ++i) {
+                const int rr = (r + i) * TR_TW + c;
+                g = fmaf(a[i], RG[rr], g);
                 bx = bx + RB[rr];
             }
-        } else {
+            dst[(size_t)(u0 + r) * W + (v0 + c)] = fmaf(-bx, ikk, g);
+        }
+    } else {
+        for (int q = threadIdx.x; q < TR_TH * TR_TW; q += TR_NT) {
+            const int r = q / TR_TW, c = q % TR_TW;
+            const int qu = u0 + r, qv = v0 + c;
+            if (qu >= H || qv >= W) continue;
+            float g = 0.f, bx = 0.f;
             for (int i = -kr; i <= kr; ++i) {
                 const int rr = (r + kr + i) * TR_TW + c;
                 g = fmaf(p.a[i + kr], RG[rr], g);
                 const int pu = qu + i;
                 if (pu >= 0 && pu < H) bx = fmaf((float)box_count(pu, qu, H, kr), RB[rr], bx);
             }
+            dst[(size_t)qu * W + qv] = fmaf(-bx, ikk, g);
         }
-        dst[(size_t)qu * W + qv] = g - bx / p.kk;
     }
 }
 
@@ -364,20 +402,33 @@ cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* 
     return cudaGetLastError();
 }
 
-cudaError_t launch_adjoint_transpose(const AdjParams& p, const float* gR, float* gI, cudaStream_t st) {
-    const size_t smem = adjoint_transpose_smem(p.krad);
-    cudaError_t e = cudaFuncSetAttribute(adjoint_transpose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <int KRT>
+cudaError_t transpose_launch(const AdjParams& p, const float* gR, float* gI, size_t smem, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(adjoint_transpose_kernel<KRT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e) return e;
     const int ntx = (p.W + TR_TW - 1) / TR_TW, nty = (p.H + TR_TH - 1) / TR_TH;
     for (int f0 = 0; f0 < p.T; f0 += 65535) {
         const int nf = std::min(65535, p.T - f0);
-        AdjParams q = p;
         dim3 grid(ntx * nty, nf);
-        adjoint_transpose_kernel<<<grid, TR_NT, smem, st>>>(q, gR + (size_t)f0 * p.H * p.W,
-                                                           gI + (size_t)f0 * p.H * p.W);
+        adjoint_transpose_kernel<KRT><<<grid, TR_NT, smem, st>>>(p, gR + (size_t)f0 * p.H * p.W,
+                                                                 gI + (size_t)f0 * p.H * p.W);
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_transpose(const AdjParams& p, const float* gR, float* gI, cudaStream_t st) {
+    const size_t smem = adjoint_transpose_smem(p.krad);
+    switch (p.krad) {
+        case 1: return transpose_launch<1>(p, gR, gI, smem, st);
+        case 2: return transpose_launch<2>(p, gR, gI, smem, st);
+        case 3: return transpose_launch<3>(p, gR, gI, smem, st);
+        case 4: return transpose_launch<4>(p, gR, gI, smem, st);
+        case 5: return transpose_launch<5>(p, gR, gI, smem, st);
+        case 6: return transpose_launch<6>(p, gR, gI, smem, st);
+        case 7: return transpose_launch<7>(p, gR, gI, smem, st);
+        default: return transpose_launch<0>(p, gR, gI, smem, st);
+    }
 }
 
 }  // namespace gt
