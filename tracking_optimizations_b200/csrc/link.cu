@@ -296,12 +296,15 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
                                 int q = w++;
                                 while (q > w0 && edst[q - 1] > d) { edst[q] = edst[q - 1]; ew[q] = ew[q - 1]; --q; }
                                 edst[q] = d; ew[q] = dist;
-                                atomicAdd(&dcnt[d], 1);
                             }
                         }
                     }
                 }
             }
+            __syncthreads();
+            // per-destination counts in a pass of their own: atomics inside
+            // the neighbour search above stall it several-fold
+            for (int q = threadIdx.x; q < ne; q += NTL) atomicAdd(&dcnt[edst[q]], 1);
             __syncthreads();
             block_scan_inplace_l(dcnt, nd + 1, warp_tot, &s_total);
             // destination lists, ascending source index (linking.rs:310-315)
