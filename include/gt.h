@@ -14,6 +14,10 @@
  *                      -> linking.rs:570-580 `linker_all` over
  *                      linking.rs:12-61 `FrameSubsetter`
  *   gt_column_names    execute_gpu.rs:197-226 `column_names`
+ *   gt_batch_file      gpu-tracking/src/lib.rs:124-200 `batch_file_rust`
+ *                      -> execute_gpu.rs:510-542 `execute_file`
+ *   gt_ets_channels, gt_file_info, gt_file_read
+ *                      lib.rs:215-232 `parse_ets` over decoderiter.rs
  *
  * Entry points with no reference counterpart (the adjoint of the locate
  * path at fixed peaks; see the declarations below):
@@ -192,6 +196,29 @@ GT_API int gt_adjoint_backward(gt_ctx* ctx, const float* d_frames, int T, int H,
 GT_API int gt_adjoint_uncertainty(gt_ctx* ctx, const float* d_frames, int T, int H, int W,
                            const gt_params* params, const int32_t* d_walk, int64_t n,
                            float gain, float read_noise, float* d_sd, void* stream);
+
+/* Locate (and link) the frames of a movie FILE (execute_gpu.rs:510-542):
+ * ".tif"/".tiff" -- every page a frame, 8- or 16-bit unsigned single-sample
+ * pages (else GT_ERR_UNSUPPORTED "Wrong bit depth"), compression none, LZW,
+ * Deflate or PackBits; ".ets" -- frames of `channel` (0 when has_channel is
+ * 0), u16 only.  Frames are decoded by host threads into pinned memory and
+ * uploaded in chunks that overlap the locate kernels.  Output as gt_batch. */
+GT_API int gt_batch_file(gt_ctx* ctx, const char* path, int has_channel, uint32_t channel,
+                  const gt_params* params, gt_table* out);
+
+/* Frame count and size of a movie file as gt_batch_file reads it (for ETS,
+ * H = dims[0] and W = dims[1], the order execute_gpu.rs:527 passes them). */
+GT_API int gt_file_info(const char* path, int has_channel, uint32_t channel, int32_t* T, int32_t* H,
+                 int32_t* W);
+
+/* The frames themselves (T * H * W u16, host), e.g. for parse_ets. */
+GT_API int gt_file_read(const char* path, int has_channel, uint32_t channel, uint16_t* out,
+                 int64_t max_values);
+
+/* Channels of an ETS file and their frame counts (up to max_channels), and
+ * its two dimensions (decoderiter.rs:133-183). */
+GT_API int gt_ets_channels(const char* path, int32_t* channels, int32_t* frames, int32_t max_channels,
+                    int32_t* nchannels, int32_t* dim0, int32_t* dim1);
 
 /* Link an (n x ncols) host f32 table whose columns 0, 2, 3 are frame, y, x
  * (link_rust's FrameSubsetter layout).  Writes n trajectory IDs. */

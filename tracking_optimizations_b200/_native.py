@@ -121,6 +121,15 @@ SIGNATURES = [
                                             ctypes.c_int, ctypes.c_int, ctypes.POINTER(GtParams), ctypes.c_void_p,
                                             ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p,
                                             ctypes.c_void_p]),
+    ("gt_batch_file", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_uint32,
+                                     ctypes.POINTER(GtParams), ctypes.POINTER(GtTable)]),
+    ("gt_file_info", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
+    ("gt_file_read", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p,
+                                    ctypes.c_int64]),
+    ("gt_ets_channels", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                       ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.POINTER(ctypes.c_int32)]),
     ("gt_batch_many_device", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GtMovie), ctypes.c_int,
                                             ctypes.c_void_p]),
     ("gt_synth_render", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgt.so")
 SOURCES = ["gt_api.cu", "locate.cu", "locate_fast.cu", "finalize.cu", "link.cu", "assemble.cu", "noalloc.cu",
-           "adjoint.cu", "synth.cu"]
+           "adjoint.cu", "synth.cu", "ingest.cpp"]
 
 # --fmad=false: the only fused multiply-adds are explicit fmaf() calls, so the
 # kernels reproduce the oracle's operation order bit for bit.
@@ -39,7 +39,7 @@ def build(force=False, verbose=False):
         if all(os.path.getmtime(s) <= t for s in srcs + hdrs):
             return LIB
     cmd = [nvcc()] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-I", CSRC,
-                                   "-o", LIB + ".tmp"] + srcs + ["-lcudart"]
+                                   "-o", LIB + ".tmp"] + srcs + ["-lcudart", "-lz"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

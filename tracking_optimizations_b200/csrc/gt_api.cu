@@ -7,6 +7,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <array>
+#include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <climits>
 #include <cstring>
 #include <string>
@@ -19,6 +24,7 @@
 
 #include "gt.h"
 #include "gt_internal.cuh"
+#include "ingest.h"
 
 namespace gt {
 __global__ void locate_tiles_kernel(const LocParams p, const MovieBufs b, int frame0);
@@ -68,6 +74,8 @@ struct gt_ctx {
     cudaStream_t side[8] = {};
     cudaEvent_t bev[20] = {};         // fork/join events
     int* h_status = nullptr;          // pinned: 8 ints per movie
+    uint16_t* h_frames = nullptr;     // pinned: decoded file frames
+    size_t h_frames_n = 0;
     size_t h_status_n = 0;
     int tune_disabled = 0;
     int batch_cap_div = 64;           // first candidate capacity of batched movies: H*W / this
@@ -569,7 +577,8 @@ int fast_division(gt_ctx* ctx, const Plan& P, FixedDiv* dn, FixedDiv* dk, bool* 
 // transfer and locate overlap.
 int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames, cudaStream_t st,
                  int* err_bits, int64_t* nrows, int* d_walk = nullptr, int64_t walk_rows = 0,
-                 const void* h_frames = nullptr, size_t elem = 0) {
+                 const void* h_frames = nullptr, size_t elem = 0,
+                 const std::function<int(int, int)>* ready = nullptr) {
     const int T = P.T;
     MovieBufs b = movie_bufs(P, w, d_frames);
     int rc = upload_tables(ctx, P, w, st);
@@ -603,6 +612,11 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
         if (ci == 0) {
             CK(cudaEventRecord(ctx->cev[8], st));
             CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->cev[8], 0));
+        }
+        if (ready) {
+            // host frames still being produced (file decode): wait for these
+            const int rr = (*ready)(f0, nf);
+            if (rr) return rr;
         }
         CK(cudaMemcpyAsync((char*)d_frames + (size_t)f0 * fbytes, (const char*)h_frames + (size_t)f0 * fbytes,
                            (size_t)nf * fbytes, cudaMemcpyHostToDevice, ctx->copy_stream));
@@ -729,7 +743,8 @@ size_t elem_size(int dtype) { return dtype == GT_U16 ? 2 : 4; }
 
 int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, int H, int W,
                  const gt_params* params, gt_table* out_tab, float* d_out, int64_t out_rows,
-                 int64_t* nrows_out, cudaStream_t st, int* d_walk = nullptr) {
+                 int64_t* nrows_out, cudaStream_t st, int* d_walk = nullptr,
+                 const std::function<int(int, int)>* ready = nullptr) {
     if (!ctx) return GT_ERR_ARG;
     ctx->err.clear();
     ctx->stats = gt_stats{};
@@ -757,7 +772,7 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
         int bits = 0;
         int64_t nrows = 0;
         rc = run_pipeline(ctx, P, w, dfr, st, &bits, &nrows, d_walk, d_walk ? out_rows : 0, host ? frames : nullptr,
-                          elem_size(dtype));
+                          elem_size(dtype), ready);
         if (rc) return rc;
         bool retry;
         rc = err_status(ctx, bits, &retry);
@@ -1027,6 +1042,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
     // pinned status words, side streams, events
     if (ctx->h_status_n < (size_t)8 * n) {
         if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->h_frames) cudaFreeHost(ctx->h_frames);
         ctx->h_status = nullptr;
         ctx->h_status_n = 0;
         CK(cudaHostAlloc((void**)&ctx->h_status, sizeof(int) * 8 * (size_t)n, cudaHostAllocDefault));
@@ -1412,6 +1428,7 @@ void gt_ctx_destroy(gt_ctx* ctx) {
     for (auto& e : ctx->cev)
         if (e) cudaEventDestroy(e);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->h_frames) cudaFreeHost(ctx->h_frames);
     for (auto& sd : ctx->side)
         if (sd) cudaStreamDestroy(sd);
     for (auto& e : ctx->bev)
@@ -1453,6 +1470,112 @@ int gt_batch(gt_ctx* ctx, const void* frames, int dtype, int T, int H, int W, co
     out->ncols = 0;
     return batch_common(ctx, frames, true, dtype, T, H, W, params, out, nullptr, 0, nullptr,
                         ctx ? ctx->stream : nullptr);
+}
+
+int gt_file_info(const char* path, int has_channel, uint32_t channel, int32_t* T, int32_t* H, int32_t* W) {
+    g_noctx_err.clear();
+    if (!T || !H || !W) { g_noctx_err = "null output"; return GT_ERR_ARG; }
+    gt::MovieFile mf;
+    std::string msg;
+    const int rc = mf.open(path, has_channel != 0, channel, &msg);
+    if (rc) { g_noctx_err = msg; return rc == 2 ? GT_ERR_UNSUPPORTED : GT_ERR_ARG; }
+    *T = mf.T; *H = mf.H; *W = mf.W;
+    return GT_OK;
+}
+
+int gt_file_read(const char* path, int has_channel, uint32_t channel, uint16_t* out, int64_t max_values) {
+    g_noctx_err.clear();
+    gt::MovieFile mf;
+    std::string msg;
+    const int rc = mf.open(path, has_channel != 0, channel, &msg);
+    if (rc) { g_noctx_err = msg; return rc == 2 ? GT_ERR_UNSUPPORTED : GT_ERR_ARG; }
+    const int64_t fpx = (int64_t)mf.H * mf.W;
+    if (!out || max_values < fpx * mf.T) { g_noctx_err = "output buffer too small"; return GT_ERR_ARG; }
+    for (int t = 0; t < mf.T; ++t)
+        if (mf.read_frame(t, out + fpx * t, &msg)) { g_noctx_err = msg; return GT_ERR_ARG; }
+    return GT_OK;
+}
+
+int gt_ets_channels(const char* path, int32_t* channels, int32_t* frames, int32_t max_channels, int32_t* nchannels,
+                    int32_t* dim0, int32_t* dim1) {
+    g_noctx_err.clear();
+    if (!nchannels || !dim0 || !dim1 || (max_channels > 0 && (!channels || !frames))) {
+        g_noctx_err = "null output";
+        return GT_ERR_ARG;
+    }
+    std::vector<std::pair<uint32_t, int>> ch;
+    uint32_t dims[2];
+    std::string msg;
+    if (gt::ets_channels(path, &ch, dims, &msg)) { g_noctx_err = msg; return GT_ERR_ARG; }
+    *nchannels = (int32_t)ch.size();
+    *dim0 = (int32_t)dims[0];
+    *dim1 = (int32_t)dims[1];
+    for (int i = 0; i < (int)ch.size() && i < max_channels; ++i) {
+        channels[i] = (int32_t)ch[i].first;
+        frames[i] = ch[i].second;
+    }
+    return GT_OK;
+}
+
+int gt_batch_file(gt_ctx* ctx, const char* path, int has_channel, uint32_t channel, const gt_params* params,
+                  gt_table* out) {
+    if (!ctx) return GT_ERR_ARG;
+    ctx->err.clear();
+    if (!params || !out) { ctx->err = "null params/output"; return GT_ERR_ARG; }
+    gt::MovieFile mf;
+    std::string msg;
+    int rc = mf.open(path, has_channel != 0, channel, &msg);
+    if (rc) { ctx->err = msg; return rc == 2 ? GT_ERR_UNSUPPORTED : GT_ERR_ARG; }
+    const size_t fpx = (size_t)mf.H * mf.W, npx = fpx * mf.T;
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->h_frames_n < npx) {
+        if (ctx->h_frames) cudaFreeHost(ctx->h_frames);
+        ctx->h_frames = nullptr;
+        ctx->h_frames_n = 0;
+        CK(cudaHostAlloc((void**)&ctx->h_frames, sizeof(uint16_t) * npx, cudaHostAllocDefault));
+        ctx->h_frames_n = npx;
+    }
+    // frames are decoded by a pool of host threads into pinned memory; each
+    // chunk's upload (and its locate launch) waits for its own frames only
+    const int T = mf.T;
+    std::vector<std::atomic<unsigned char>> done(T);
+    for (auto& d : done) d.store(0);
+    std::atomic<int> next{0}, failed{0};
+    std::mutex mu;
+    std::condition_variable cv;
+    std::string err;
+    uint16_t* dst = ctx->h_frames;
+    auto worker = [&]() {
+        std::string m;
+        for (int t = next.fetch_add(1); t < T && !failed.load(); t = next.fetch_add(1)) {
+            if (mf.read_frame(t, dst + fpx * t, &m)) {
+                std::lock_guard<std::mutex> lk(mu);
+                if (!failed.exchange(1)) err = m;
+                cv.notify_all();
+                return;
+            }
+            done[t].store(1);
+            std::lock_guard<std::mutex> lk(mu);
+            cv.notify_all();
+        }
+    };
+    const int nthr = (int)std::max(1u, std::min<unsigned>({std::thread::hardware_concurrency(), 16u, (unsigned)T}));
+    std::vector<std::thread> pool;
+    for (int i = 0; i < nthr; ++i) pool.emplace_back(worker);
+    const std::function<int(int, int)> ready = [&](int f0, int nf) -> int {
+        std::unique_lock<std::mutex> lk(mu);
+        for (int t = f0; t < f0 + nf; ++t) {
+            cv.wait(lk, [&] { return done[t].load() || failed.load(); });
+            if (failed.load()) return GT_ERR_ARG;
+        }
+        return GT_OK;
+    };
+    rc = batch_common(ctx, dst, true, GT_U16, T, mf.H, mf.W, params, out, nullptr, 0, nullptr, ctx->stream, nullptr,
+                      &ready);
+    failed.store(failed.load() | (rc ? 2 : 0));
+    for (auto& th : pool) th.join();
+    if (rc == GT_ERR_ARG && !err.empty()) ctx->err = err;
+    return rc;
 }
 
 int gt_batch_device(gt_ctx* ctx, const void* d_frames, int dtype, int T, int H, int W,

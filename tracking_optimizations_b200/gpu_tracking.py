@@ -8,11 +8,14 @@ Same names, positional order and defaults:
              cpu_processed, sig_radius, bg_radius, gap_radius)
       -> (float32 array [rows, cols], [(name, type), ...])
   link_rust(pyarr, search_range, memory=None) -> uint64 array
+  batch_file_rust(filename, diameter, channel=None, ...) -> as batch_rust
+  parse_ets(path) -> {channel: uint16 array}
 The reference accepts float32 frames only (lib.rs:50); uint16 frames are
 accepted as well.  Unsupported options raise NotImplementedError as the
 reference's `not_implemented!` does (lib.rs:28-39, 73-74).
 """
 import ctypes
+import os
 import weakref
 
 import numpy as np
@@ -112,9 +115,68 @@ def batch_device(frames, diameter, **params):
     raise RuntimeError("row count changed between two identical calls")
 
 
-def batch_file_rust(filename, diameter, channel=None, *args, **kwargs):
-    """File ingest (TIFF/ETS) is not part of this build's hot path."""
-    raise NotImplementedError("batch_file_rust: file ingest is not implemented in the B200 build")
+def batch_file_rust(filename, diameter, channel=None, minmass=None, maxsize=None, separation=None, noise_size=None,
+                    smoothing_size=None, threshold=None, invert=None, percentile=None, topn=None, preprocess=None,
+                    max_iterations=None, characterize=None, filter_close=None, search_range=None, memory=None,
+                    cpu_processed=None, sig_radius=None, bg_radius=None, gap_radius=None, device=0):
+    """Locate (and link) the frames of a .tif/.tiff or .ets movie file
+    (lib.rs:124-200 -> execute_gpu.rs:510-542); `channel` selects the ETS
+    channel (0 by default) and is ignored for TIFF."""
+    vals = dict(minmass=minmass, maxsize=maxsize, separation=separation, noise_size=noise_size,
+                smoothing_size=smoothing_size, threshold=threshold, invert=invert, percentile=percentile,
+                topn=topn, preprocess=preprocess, max_iterations=max_iterations, characterize=characterize,
+                filter_close=filter_close, search_range=search_range, memory=memory,
+                cpu_processed=cpu_processed, sig_radius=sig_radius, bg_radius=bg_radius,
+                gap_radius=gap_radius)
+    params = _native.make_params(diameter, **vals)
+    lib = _native.load()
+    ctx = _native.context(device)
+    tab = _native.GtTable()
+    st = lib.gt_batch_file(ctx, os.fsencode(filename), 0 if channel is None else 1,
+                           0 if channel is None else int(channel), ctypes.byref(params), ctypes.byref(tab))
+    _native.check(st, ctx)
+    try:
+        n, c = tab.nrows, tab.ncols
+        cols = [(tab.names[i].value.decode(), tab.types[i].value.decode()) for i in range(c)]
+        out = _adopt_table(lib, tab, n, c)
+    except BaseException:
+        lib.gt_table_free(ctypes.byref(tab))
+        raise
+    return out, cols
+
+
+def read_file(path, channel=None):
+    """The frames of a movie file as gt_batch_file reads them: (T, H, W)
+    uint16 (for ETS, H = dims[0] and W = dims[1])."""
+    lib = _native.load()
+    T, H, W = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    hc, ch = (0, 0) if channel is None else (1, int(channel))
+    _native.check(lib.gt_file_info(os.fsencode(path), hc, ch, ctypes.byref(T), ctypes.byref(H), ctypes.byref(W)), None)
+    out = np.empty((T.value, H.value, W.value), np.uint16)
+    _native.check(lib.gt_file_read(os.fsencode(path), hc, ch, out.ctypes.data_as(ctypes.c_void_p), out.size), None)
+    return out
+
+
+def parse_ets(path):
+    """{channel: uint16 array (frames, dims[1], dims[0])} of an ETS file
+    (lib.rs:215-232)."""
+    lib = _native.load()
+    n, d0, d1 = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    _native.check(lib.gt_ets_channels(os.fsencode(path), None, None, 0, ctypes.byref(n), ctypes.byref(d0),
+                                      ctypes.byref(d1)), None)
+    chans = np.empty(n.value, np.int32)
+    frames = np.empty(n.value, np.int32)
+    _native.check(lib.gt_ets_channels(os.fsencode(path), chans.ctypes.data_as(ctypes.c_void_p),
+                                      frames.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n),
+                                      ctypes.byref(d0), ctypes.byref(d1)), None)
+    out = {}
+    for c, f in zip(chans.tolist(), frames.tolist()):
+        a = np.empty((f, d1.value, d0.value), np.uint16)
+        if f:
+            _native.check(lib.gt_file_read(os.fsencode(path), 1, c, a.ctypes.data_as(ctypes.c_void_p), a.size),
+                          None)
+        out[c] = a
+    return out
 
 
 def link_rust(pyarr, search_range, memory=None, device=0):
