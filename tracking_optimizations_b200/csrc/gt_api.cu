@@ -827,7 +827,10 @@ struct BatchMovie {
     size_t off = 0;
     bool fast = false;
     FixedDiv dn{}, dk{};
-    int link_slot = -1;  // index among the linked movies
+    int link_slot = -1;  // index among the movies of the shared linker launch
+    bool solo = false;   // linked by its own cooperative launch (large movie)
+    LinkBufs solo_L{};
+    int solo_grid = 0;
 };
 
 struct BatchShared {
@@ -838,6 +841,7 @@ struct BatchShared {
     int* d_passes = nullptr;
     int* d_status = nullptr;  // 8 ints per movie: err[0..3], nrows
     int nlink = 0, max_passes = 0, link_grid = 0;
+    int nsolo = 0, solo_grid = 0;
     int launches = 0;
 };
 
@@ -979,7 +983,7 @@ int enqueue_batch(gt_ctx* ctx, std::vector<BatchMovie>& B, gt_movie* mv, int n, 
         CK(cudaStreamWaitEvent(st, ctx->bev[1 + k], 0));
     }
     if (S.nlink > 0) {
-        CK(cudaMemsetAsync(S.d_ndirty, 0, sizeof(int) * (S.max_passes + 2), st));
+        CK(cudaMemsetAsync(S.d_ndirty, 0, sizeof(int) * (size_t)(S.max_passes + 2) * S.nlink, st));
         const LinkBufs* Ls = S.d_L;
         const int* mem = S.d_mem;
         const int* fst = S.d_fstart;
@@ -988,6 +992,20 @@ int enqueue_batch(gt_ctx* ctx, std::vector<BatchMovie>& B, gt_movie* mv, int n, 
         int* ps = S.d_passes;
         void* args[] = {(void*)&Ls, (void*)&mem, (void*)&fst, &nm, &mp, &nd, &ps};
         CK(cudaLaunchCooperativeKernel((const void*)link_fixpoint_multi_kernel, dim3(S.link_grid), dim3(256), args,
+                                       LINK_POOL_BYTES, st));
+        S.launches += 1;
+    }
+    for (int i = 0; i < n; ++i) {
+        if (!B[i].solo) continue;
+        BatchMovie& bm = B[i];
+        CK(cudaMemsetAsync(bm.w.ndirty, 0, sizeof(int) * (bm.P.T + 2), st));
+        LinkBufs L = bm.solo_L;
+        int memory = (int)bm.P.r.memory, max_passes = bm.P.T + 1, rounds = 0;
+        int* nd = bm.w.ndirty;
+        int* ps = bm.w.err + 1;
+        unsigned long long* ph = bm.w.phase_ns;
+        void* args[] = {&L, &memory, &max_passes, &rounds, &nd, &ps, &ph};
+        CK(cudaLaunchCooperativeKernel((const void*)link_fixpoint_kernel, dim3(bm.solo_grid), dim3(256), args,
                                        LINK_POOL_BYTES, st));
         S.launches += 1;
     }
@@ -1065,12 +1083,39 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
             bm.fast = ok;
         }
     }
-    // linked movies: shared slot strides
+    // linked movies: a movie whose per-block scratch would cap the linker
+    // grid below full residency is linked by its own launch (as in the
+    // one-movie path); the others share one launch whose blocks share one
+    // scratch pool (slot strides of the largest of them)
     BatchShared S;
-    long long st_s = 1, st_s1 = 1, st_p1 = 1, st_n = 1, st_e = 1, st_h = 64;
+    const size_t budget = (size_t)6 << 30;
+    auto slot_bytes = [](long long s_, long long s1, long long p1, long long n_, long long e_, long long h_) {
+        return (size_t)(4 * (3 * s_ + s1) + 8 * e_ * 2 + 4 * p1 + 4 * 4 * n_ + n_ + 16 * n_ + 4 + 8 * h_);
+    };
+    int per_sm_multi = 0, per_sm_solo = 0;
+    CK(cudaFuncSetAttribute(link_fixpoint_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, LINK_POOL_BYTES));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_multi, link_fixpoint_multi_kernel, 256, LINK_POOL_BYTES));
+    CK(cudaFuncSetAttribute(link_fixpoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, LINK_POOL_BYTES));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_solo, link_fixpoint_kernel, 256, LINK_POOL_BYTES));
+    const size_t full_grid = (size_t)std::max(1, per_sm_multi) * ctx->num_sms;
+    long long st_s = 1, st_s1 = 1, st_p1 = 1, st_n = 1, st_e = 1, st_h = 64;        // shared launch
+    long long bt_s = 1, bt_s1 = 1, bt_p1 = 1, bt_n = 1, bt_e = 1, bt_h = 64;        // solo launches
     for (int i = 0; i < n; ++i) {
         const Plan& P = B[i].P;
         if (!P.link) continue;
+        const size_t own = slot_bytes(P.cap_s, (long long)P.cap_s + 1, (long long)P.cap_p + 1,
+                                      (long long)P.cap_s + P.cap_p, P.cap_e, P.hsize);
+        if (budget / own < full_grid) {
+            B[i].solo = true;
+            ++S.nsolo;
+            bt_s = std::max<long long>(bt_s, P.cap_s);
+            bt_s1 = std::max<long long>(bt_s1, (long long)P.cap_s + 1);
+            bt_p1 = std::max<long long>(bt_p1, (long long)P.cap_p + 1);
+            bt_n = std::max<long long>(bt_n, (long long)P.cap_s + P.cap_p);
+            bt_e = std::max<long long>(bt_e, P.cap_e);
+            bt_h = std::max<long long>(bt_h, P.hsize);
+            continue;
+        }
         B[i].link_slot = S.nlink++;
         st_s = std::max<long long>(st_s, P.cap_s);
         st_s1 = std::max<long long>(st_s1, (long long)P.cap_s + 1);
@@ -1080,15 +1125,12 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         st_h = std::max<long long>(st_h, P.hsize);
         S.max_passes = std::max(S.max_passes, P.T + 1);
     }
-    if (S.nlink > 0) {
-        CK(cudaFuncSetAttribute(link_fixpoint_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, LINK_POOL_BYTES));
-        int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_multi_kernel, 256, LINK_POOL_BYTES));
-        const size_t per_slot = 4 * (3 * st_s + st_s1) + 8 * st_e * 2 + 4 * st_p1 + 4 * 4 * st_n + st_n + 16 * st_n +
-                                4 + 8 * st_h;
-        const size_t budget = (size_t)6 << 30;
-        S.link_grid = (int)std::max<size_t>(1, std::min<size_t>((size_t)per_sm * ctx->num_sms, budget / per_slot));
-    }
+    if (S.nlink > 0)
+        S.link_grid = (int)std::max<size_t>(1, std::min<size_t>(full_grid,
+                                                                budget / slot_bytes(st_s, st_s1, st_p1, st_n, st_e, st_h)));
+    if (S.nsolo > 0)
+        S.solo_grid = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(1, per_sm_solo) * ctx->num_sms,
+                                                                budget / slot_bytes(bt_s, bt_s1, bt_p1, bt_n, bt_e, bt_h)));
     // arena layout: movies, link pool, shared arrays
     size_t total = 0;
     for (int i = 0; i < n; ++i) {
@@ -1099,20 +1141,44 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         total += carve(Pc, nullptr, &w, 0, true, false);
         total = (total + 255) / 256 * 256;
     }
-    const size_t G = S.link_grid;
+    const size_t G = S.link_grid, GB = S.solo_grid;
     Carver pc{nullptr};
+    auto slots = [](Carver& c, Work& pw, size_t g, long long s_, long long s1, long long p1, long long n_,
+                    long long e_, long long h_) {
+        pw.s_y = c.take<float>(g * s_); pw.s_x = c.take<float>(g * s_); pw.s_h = c.take<int>(g * s_);
+        pw.s_deg = c.take<int>(g * s1); pw.e_dst = c.take<int>(g * e_); pw.e_w = c.take<float>(g * e_);
+        pw.d_cnt = c.take<int>(g * p1); pw.d_src = c.take<int>(g * e_); pw.d_w = c.take<float>(g * e_);
+        pw.uf = c.take<int>(g * n_); pw.c_nd = c.take<int>(g * n_); pw.c_ns = c.take<int>(g * n_);
+        pw.c_min = c.take<int>(g * n_); pw.vis = c.take<unsigned char>(g * n_);
+        pw.work = c.take<int>(g * 4 * n_); pw.bump = c.take<int>(g); pw.hkey = c.take<int>(g * h_);
+        pw.hval = c.take<int>(g * h_);
+    };
+    // solo launches run one after another: each lays out its own grid of
+    // slots with its own strides at the start of one shared region
+    size_t big_bytes = 0;
+    for (int i = 0; i < n; ++i) {
+        if (!B[i].solo) continue;
+        const Plan& P = B[i].P;
+        const size_t own = slot_bytes(P.cap_s, (long long)P.cap_s + 1, (long long)P.cap_p + 1,
+                                      (long long)P.cap_s + P.cap_p, P.cap_e, P.hsize);
+        B[i].solo_grid = (int)std::max<size_t>(1, std::min<size_t>({(size_t)P.T,
+                                                                   (size_t)std::max(1, per_sm_solo) * ctx->num_sms,
+                                                                   budget / own}));
+        Carver dry{nullptr};
+        Work wd{};
+        slots(dry, wd, B[i].solo_grid, P.cap_s, (long long)P.cap_s + 1, (long long)P.cap_p + 1,
+              (long long)P.cap_s + P.cap_p, P.cap_e, P.hsize);
+        big_bytes = std::max(big_bytes, dry.off);
+    }
+    char* big_base = nullptr;
+    (void)GB;
     auto pool_layout = [&](Carver& c, Work& pw) {
-        pw.s_y = c.take<float>(G * st_s); pw.s_x = c.take<float>(G * st_s); pw.s_h = c.take<int>(G * st_s);
-        pw.s_deg = c.take<int>(G * st_s1); pw.e_dst = c.take<int>(G * st_e); pw.e_w = c.take<float>(G * st_e);
-        pw.d_cnt = c.take<int>(G * st_p1); pw.d_src = c.take<int>(G * st_e); pw.d_w = c.take<float>(G * st_e);
-        pw.uf = c.take<int>(G * st_n); pw.c_nd = c.take<int>(G * st_n); pw.c_ns = c.take<int>(G * st_n);
-        pw.c_min = c.take<int>(G * st_n); pw.vis = c.take<unsigned char>(G * st_n);
-        pw.work = c.take<int>(G * 4 * st_n); pw.bump = c.take<int>(G); pw.hkey = c.take<int>(G * st_h);
-        pw.hval = c.take<int>(G * st_h);
+        slots(c, pw, G, st_s, st_s1, st_p1, st_n, st_e, st_h);
+        big_base = c.take<char>(big_bytes);
         S.d_L = c.take<LinkBufs>(std::max(1, S.nlink));
         S.d_mem = c.take<int>(std::max(1, S.nlink));
         S.d_fstart = c.take<int>(std::max(1, S.nlink));
-        S.d_ndirty = c.take<int>(S.max_passes + 2);
+        S.d_ndirty = c.take<int>((size_t)(S.max_passes + 2) * std::max(1, S.nlink));
         S.d_passes = c.take<int>(1);
         S.d_status = c.take<int>(8 * (size_t)n);
     };
@@ -1182,6 +1248,23 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         CK(cudaMemcpyAsync(S.d_mem, hm.data(), sizeof(int) * S.nlink, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(S.d_fstart, hf.data(), sizeof(int) * S.nlink, cudaMemcpyHostToDevice, st));
     }
+    for (int i = 0; i < n; ++i) {
+        if (!B[i].solo) continue;
+        const Plan& P = B[i].P;
+        Work pool_big{};
+        Carver cb{big_base};
+        slots(cb, pool_big, B[i].solo_grid, P.cap_s, (long long)P.cap_s + 1, (long long)P.cap_p + 1,
+              (long long)P.cap_s + P.cap_p, P.cap_e, P.hsize);
+        LinkBufs L = link_bufs(B[i].P, B[i].w);
+        L.nslot = B[i].solo_grid;
+        L.s_y = pool_big.s_y; L.s_x = pool_big.s_x; L.s_h = pool_big.s_h; L.s_deg = pool_big.s_deg;
+        L.e_dst = pool_big.e_dst; L.e_w = pool_big.e_w; L.d_cnt = pool_big.d_cnt; L.d_src = pool_big.d_src;
+        L.d_w = pool_big.d_w; L.uf = pool_big.uf; L.c_nd = pool_big.c_nd; L.c_ns = pool_big.c_ns;
+        L.c_min = pool_big.c_min; L.vis = pool_big.vis; L.work = pool_big.work; L.bump = pool_big.bump;
+        L.hkey = pool_big.hkey; L.hval = pool_big.hval;
+        L.lsm_bytes = LINK_POOL_BYTES;  // slot strides: the movie's own (link_bufs)
+        B[i].solo_L = L;
+    }
     if (!replay) {
         if (ctx->batch_exec) { cudaGraphExecDestroy(ctx->batch_exec); ctx->batch_exec = nullptr; }
         ctx->batch_key.clear();
@@ -1242,7 +1325,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
             const Plan& P = B[i].P;
             cnt += (P.T + 65534) / 65535 + 3 + (P.link ? 2 : 0) + 1;
         }
-        S.launches = cnt + (S.nlink > 0 ? 1 : 0);
+        S.launches = cnt + (S.nlink > 0 ? 1 : 0) + S.nsolo;
     }
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(cudaStreamSynchronize(st));
@@ -1253,6 +1336,8 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         CK(cudaMemcpy(&passes, S.d_passes, sizeof(int), cudaMemcpyDeviceToHost));
         ctx->stats.link_iterations = passes;
     }
+    for (int i = 0; i < n; ++i)
+        if (B[i].solo) ctx->stats.link_iterations = std::max(ctx->stats.link_iterations, ctx->h_status[8 * i + 1]);
     // per-movie status; capacity overflows are rerun through the plain path
     std::vector<int> status(ctx->h_status, ctx->h_status + 8 * (size_t)n);
     gt_stats keep = ctx->stats;

@@ -679,19 +679,30 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_multi_kernel(const LinkB
         link_frames_body(Ls[m], 0, t0_of(m), G);
         any_mem |= memory[m] > 0 && Ls[m].T > 2;
     }
+    // ndirty[k * nm + m]: frames of movie m changed by pass k.  A movie
+    // whose memory entries did not change in a pass is at its fixed point
+    // (movies are independent): later passes skip it.
+    auto active = [&](int m, int k) {
+        return memory[m] > 0 && Ls[m].T > 2 && (k == 1 || *(volatile int*)(ndirty + (k - 1) * nm + m) > 0);
+    };
     int k = 0;
     if (any_mem) {
         for (k = 1; k <= max_passes; ++k) {
             grid.sync();
-            for (int m = 0; m < nm; ++m) roots_reset(Ls[m]);
-            grid.sync();
-            for (int m = 0; m < nm; ++m) roots_walk(Ls[m]);
+            for (int m = 0; m < nm; ++m)
+                if (active(m, k)) roots_reset(Ls[m]);
             grid.sync();
             for (int m = 0; m < nm; ++m)
-                if (memory[m] > 0 && Ls[m].T > 2) memory_body(Ls[m], memory[m], ndirty + k, t0_of(m), G);
+                if (active(m, k)) roots_walk(Ls[m]);
             grid.sync();
-            if (*(volatile int*)(ndirty + k) == 0) break;
-            for (int m = 0; m < nm; ++m) link_frames_body(Ls[m], 1, t0_of(m), G);
+            for (int m = 0; m < nm; ++m)
+                if (active(m, k)) memory_body(Ls[m], memory[m], ndirty + k * nm + m, t0_of(m), G);
+            grid.sync();
+            int total = 0;
+            for (int m = 0; m < nm; ++m) total += *(volatile int*)(ndirty + k * nm + m);
+            if (total == 0) break;
+            for (int m = 0; m < nm; ++m)
+                if (*(volatile int*)(ndirty + k * nm + m) > 0) link_frames_body(Ls[m], 1, t0_of(m), G);
         }
     }
     grid.sync();
