@@ -114,3 +114,21 @@ def test_batch_rejects_bad_movie(torch, movies):
     bad = (movies[0][0], dict(diameter=7, percentile=50.0))
     with pytest.raises(NotImplementedError, match="percentile"):
         batch_many([movies[1], bad])
+
+
+def test_large_movie_linked_by_its_own_launch(torch, movies):
+    # a dense 2048^2 movie with memory 3: its linker scratch would cap a
+    # shared launch, so it is linked alone; the small movie shares the
+    # multi-movie launch
+    from tracking_optimizations_b200.batched import batch_many, output_buffers
+
+    spec = synth.scaled(synth.DENSE_LINK, frames=6, seed=61)
+    dense = (synth.make_movie_device(spec), dict(spec.params))
+    mix = [movies[0], dense, movies[4]]
+    want = _plain(torch, mix)
+    outs = output_buffers(mix)
+    for rep in range(2):
+        got, st = batch_many(mix, return_stats=True, outs=outs)
+        assert st["batch_fallbacks"] == 0
+        for i, ((tab, _), w) in enumerate(zip(got, want)):
+            np.testing.assert_array_equal(tab.cpu().numpy(), w, err_msg=f"movie {i} (call {rep})")
