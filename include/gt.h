@@ -87,7 +87,8 @@ typedef struct gt_params {
 
 /* Result of gt_batch: nrows x ncols row-major f32 (the reference returns the
  * same matrix plus its column list, lib.rs:119-120).  `data` is owned by the
- * library; release it with gt_table_free. */
+ * library (page-locked host memory where the driver grants it, reused by
+ * later calls once released); release it with gt_table_free. */
 typedef struct gt_table {
     float* data;
     int64_t nrows;

@@ -220,3 +220,22 @@ def test_full_size_dense_linking(gpu):
     assert_tables_equal(got, want, None)
     print(f"dense linking: {got[0].shape[0]} rows, {int(got[0][:, 4].max()) + 1} trajectories, "
           f"link passes {st['link_iterations']}, link {st['ms_link']:.2f} ms")
+
+
+def test_tables_alive_across_calls_keep_their_contents():
+    # host tables come from a pool of page-locked blocks: a table still
+    # referenced must never be handed to a later call
+    spec = synth.scaled(synth.PLAIN_SMALL, frames=6, seed=5)
+    movie = synth.make_movie(spec)
+    other = synth.make_movie(synth.scaled(synth.PLAIN_SMALL, frames=6, seed=6))
+    params = dict(spec.params)
+    d = params.pop("diameter")
+    want_a, _ = oracle.batch(movie, d, nthreads=NTHREADS, **params)
+    want_b, _ = oracle.batch(other, d, nthreads=NTHREADS, **params)
+    held = []
+    for i in range(6):
+        held.append((i, batch_rust(movie if i % 2 == 0 else other, d, **params)[0]))
+        if i == 3:
+            del held[:2]  # released blocks go back to the pool and are reused
+    for i, tab in held:
+        np.testing.assert_array_equal(tab, want_a if i % 2 == 0 else want_b, err_msg=f"call {i}")

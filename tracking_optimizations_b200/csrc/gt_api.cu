@@ -599,9 +599,10 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
         fast = ok;  // otherwise the generic kernel (IEEE division)
     }
     ctx->stats.locate_kernel = fast ? 1 : 0;
-    // frame chunks: up to 8 for host frames (copy/locate overlap), else
-    // as large as the grid allows
-    const int chunk = h_frames ? std::min(65535, std::max(16, (T + 7) / 8)) : 65535;
+    // frame chunks: up to 16 for host frames (copy/locate overlap; the
+    // locate of the last chunk is what remains after the copy), else as
+    // large as the grid allows
+    const int chunk = h_frames ? std::min(65535, std::max(16, (T + 15) / 16)) : 65535;
     const size_t fbytes = (size_t)P.H * P.W * elem;
     int ci = 0;
     auto stage = [&](int f0, int nf) -> int {
@@ -741,6 +742,70 @@ int err_status(gt_ctx* ctx, int bits, bool* retry) {
 
 size_t elem_size(int dtype) { return dtype == GT_U16 ? 2 : 4; }
 
+// Host tables (gt_table.data) live in page-locked memory, so the
+// device->host copy of a table runs at full PCIe speed and touches no fresh
+// pages.  Released tables go back to a small process-wide pool (gt_table_free
+// has no context) and are reused by later calls of a similar size; memory
+// that cannot be page-locked falls back to malloc.
+struct TablePool {
+    std::mutex m;
+    std::vector<std::pair<void*, size_t>> idle;  // page-locked blocks not in use
+    std::map<void*, size_t> locked;               // every page-locked block handed out or idle
+    size_t idle_bytes = 0;
+};
+TablePool& table_pool() {
+    static TablePool* pool = new TablePool();  // never destroyed: tables may be freed at exit
+    return *pool;
+}
+constexpr size_t TABLE_IDLE_MAX_BLOCKS = 4;
+constexpr size_t TABLE_IDLE_MAX_BYTES = (size_t)1 << 30;
+
+float* table_alloc(size_t bytes) {
+    TablePool& tp = table_pool();
+    {
+        std::lock_guard<std::mutex> g(tp.m);
+        int best = -1;
+        for (int i = 0; i < (int)tp.idle.size(); ++i) {
+            const size_t sz = tp.idle[i].second;
+            if (sz >= bytes && sz <= 2 * bytes + ((size_t)2 << 20) && (best < 0 || sz < tp.idle[best].second))
+                best = i;
+        }
+        if (best >= 0) {
+            void* q = tp.idle[best].first;
+            tp.idle_bytes -= tp.idle[best].second;
+            tp.idle.erase(tp.idle.begin() + best);
+            return (float*)q;
+        }
+    }
+    const size_t sz = (bytes + ((size_t)2 << 20) - 1) / ((size_t)2 << 20) * ((size_t)2 << 20);
+    void* q = nullptr;
+    if (cudaHostAlloc(&q, sz, cudaHostAllocPortable) == cudaSuccess && q) {
+        std::lock_guard<std::mutex> g(tp.m);
+        tp.locked[q] = sz;
+        return (float*)q;
+    }
+    cudaGetLastError();
+    return (float*)std::malloc(bytes);
+}
+
+void table_release(void* q) {
+    if (!q) return;
+    TablePool& tp = table_pool();
+    std::lock_guard<std::mutex> g(tp.m);
+    auto it = tp.locked.find(q);
+    if (it == tp.locked.end()) {
+        std::free(q);
+        return;
+    }
+    if (tp.idle.size() < TABLE_IDLE_MAX_BLOCKS && tp.idle_bytes + it->second <= TABLE_IDLE_MAX_BYTES) {
+        tp.idle.push_back({q, it->second});
+        tp.idle_bytes += it->second;
+        return;
+    }
+    tp.locked.erase(it);
+    cudaFreeHost(q);  // an error here (runtime already unloading at exit) is harmless
+}
+
 int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, int H, int W,
                  const gt_params* params, gt_table* out_tab, float* d_out, int64_t out_rows,
                  int64_t* nrows_out, cudaStream_t st, int* d_walk = nullptr,
@@ -789,7 +854,7 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
                 std::snprintf(out_tab->names[i], sizeof(out_tab->names[i]), "%s", P.names[i].c_str());
                 std::snprintf(out_tab->types[i], sizeof(out_tab->types[i]), "%s", P.types[i].c_str());
             }
-            out_tab->data = (float*)std::malloc(sizeof(float) * (size_t)std::max<int64_t>(1, nrows) * ncols);
+            out_tab->data = table_alloc(sizeof(float) * (size_t)std::max<int64_t>(1, nrows) * ncols);
             if (!out_tab->data) { ctx->err = "host allocation failed"; return GT_ERR_OOM; }
             if (nrows > 0) {
                 CK(cudaMemcpyAsync(out_tab->data, w.out, sizeof(float) * (size_t)nrows * ncols,
@@ -1782,7 +1847,7 @@ int gt_ctx_set_option(gt_ctx* ctx, const char* key, int value) {
 }
 
 void gt_table_free(gt_table* table) {
-    if (table && table->data) { std::free(table->data); table->data = nullptr; }
+    if (table && table->data) { table_release(table->data); table->data = nullptr; }
 }
 
 int gt_last_stats(const gt_ctx* ctx, gt_stats* out) {

@@ -9,7 +9,7 @@
 // centroid radius RC with diameter 2*RC + 1), so the whole tile geometry is
 // known at compile time: every shared-memory offset is an immediate and
 // every loop has a constant trip count.  One CTA per (frame, TH0 x 64 output
-// tile), 256 threads:
+// tile), 256 or 512 threads:
 //   0. the uint16 tile plus halo is staged by one TMA load (zero fill
 //      outside the frame) into U[RH][RW];
 //   1. U -> Rp: f32, rows interleaved in pairs (float2 = rows 2p, 2p+1);
@@ -19,8 +19,10 @@
 //      divides by the Gaussian norm and k^2, clips at 0 -> P2 (row pairs);
 //   4. row max over the dilation window (register sliding max) -> RM2;
 //   5. column max of RM2 compared with the centre -> local-max flags;
-//   6. flagged pixels are compacted in raster order; the tile's candidates
-//      share one warp for the walk, the features and the emission.
+//   6. each warp lists the flagged pixels of its own tile rows in raster
+//      order (ballots), walks them one per lane, computes the features and
+//      emits the records with one slot atomic per 32 candidates; warps do
+//      not wait for each other.
 // Row strides of the pair arrays are odd (in 8-byte units), so every
 // lane-per-row access is bank-conflict free.
 #include <cuda.h>
@@ -41,7 +43,6 @@ constexpr int FNT = 256;  // threads of a 32-row tile
 // output row) keep 16 warps per SM slot at 2 CTAs per SM
 __host__ __device__ constexpr int fast_threads(int th) { return th == 32 ? FNT : 2 * FNT; }
 constexpr int FM = 8;     // outputs per thread item
-constexpr int FCMAX = 512;
 
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int round8(int x) { return (x + 7) / 8 * 8; }
@@ -78,7 +79,7 @@ struct Geo {
     static constexpr int RPA = 4 * NRQ + KR;  // Gp/Bp row pairs allocated
     static constexpr int SZ_RP = align128(cmax(RP * RPS * 8, 4 * NRQ * P2S * 8));
     static constexpr int SZ_GP = align128(cmax(cmax(RPA * GPS * 8, (PP + 1) * RMS * 8), TH0 * FT * 4));
-    static constexpr int SZ_BP = align128(cmax(cmax(RPA * GPS * 8, RH * RW * 2), TH0 * FT + 6 * 4 * FCMAX));
+    static constexpr int SZ_BP = align128(cmax(cmax(RPA * GPS * 8, RH * RW * 2), TH0 * FT));
     static constexpr int K = circle_size(RC);
     static constexpr int SZ_TAB = align128(K * 8);
     static constexpr int OFF_GP = SZ_RP;
@@ -284,10 +285,8 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     constexpr int HP = G::HP, HX = G::HX;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int warp_tot[NTK / 32];
-    __shared__ int s_total, s_base, s_fail;
+    __shared__ int s_fail;
     __shared__ int rowcount[TH0];
-    __shared__ int rowstart[TH0];
 
     const int tid = threadIdx.x;
     const int tile = blockIdx.x;
@@ -307,12 +306,6 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     float2* RM2 = Gp;                           // after the column pass
     int* clist = (int*)Gp;                      // after the local-max pass
     unsigned char* flags = (unsigned char*)Bp;  // after the column pass
-    float* wy = (float*)(smem + G::OFF_BP + TH0 * FT);
-    float* wx = wy + FCMAX;
-    float* wm = wx + FCMAX;
-    int* wst = (int*)(wm + FCMAX);
-    unsigned int* wlp = (unsigned int*)(wst + FCMAX);  // last-read pixel (u << 16 | v)
-    unsigned int* wfp = wlp + FCMAX;                   // final position (u << 16 | v)
     float2* sc = (float2*)(smem + G::OFF_TAB);  // (sin2, cos2) of the d/2 circle
 
     // ---- 0. stage the raw tile ----
@@ -348,10 +341,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         }
         __syncthreads();
     }
-    if (tid < TH0) {
-        rowstart[tid] = 0x7fffffff;
-        rowcount[tid] = 0;
-    }
+    if (tid < TH0) rowcount[tid] = 0;
     if (p.cpu_processed)
         for (int k = tid; k < G::K; k += NTK)
             sc[k] = make_float2(__ldg(b.char_tab + 3 * k + 1), __ldg(b.char_tab + 3 * k + 2));
@@ -532,103 +522,99 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     }
     __syncthreads();
 
-    // ---- 6. raster-order compaction, walks, emission ----
-    constexpr int CHUNK = TH0 * FT / NTK;  // 8 or 16 flags per thread
-    const int q0 = tid * CHUNK;
-    int mine = 0;
-    unsigned char fl[CHUNK];
+    // ---- 6. per-warp compaction, walks and emission ----
+    // Warp w owns tile rows [w * RPW, (w + 1) * RPW): its candidates are
+    // listed in raster order by ballots, walked one per lane, and emitted
+    // with slots from one atomic per round of 32, so no warp waits for
+    // another.  rowrank = rank among the emitted records of the (row, tile)
+    // segment, as finalize_kernel expects.
+    constexpr int NW = NTK / 32;
+    constexpr int RPW = TH0 / NW;
+    static_assert(RPW * NW == TH0 && FT == 64, "warp row ownership");
+    const int warp = tid >> 5, lane = tid & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int* cl = clist + warp * (RPW * FT);
+    int nc = 0;
 #pragma unroll
-    for (int i = 0; i < CHUNK; ++i) {
-        fl[i] = flags[q0 + i];
-        mine += fl[i];
+    for (int rr = 0; rr < RPW; ++rr) {
+        const int r = warp * RPW + rr;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int q = r * FT + h * 32 + lane;
+            const bool f = flags[q] != 0;
+            const unsigned bal = __ballot_sync(0xffffffffu, f);
+            if (f) cl[nc + __popc(bal & lt)] = q;
+            nc += __popc(bal);
+        }
     }
-    int pos = block_excl_scan<NTK>(mine, warp_tot, &s_total);
-    const int ncand = s_total;
-#pragma unroll
-    for (int i = 0; i < CHUNK; ++i)
-        if (fl[i]) clist[pos++] = q0 + i;
-    __syncthreads();
+    __syncwarp();
 
     P2Acc<G> acc{(const float*)P2, py0, px0};
     const unsigned short* frame = (const unsigned short*)b.frames + (size_t)t * H * W;
     GRawAcc racc{frame, W};
-    int emitted = 0;
-    for (int r0 = 0; r0 < ncand; r0 += FCMAX) {
-        const int nr = min(FCMAX, ncand - r0);
-        for (int c = tid; c < nr; c += NTK) {
-            const int q = clist[r0 + c];
-            const int u0 = ty0 + q / FT, v0 = tx0 + q % FT;
-            int st;
-            float y = 0.f, x = 0.f, m = 0.f;
-            unsigned int lp = 0, fp = 0;
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+        const int c = c0 + lane;
+        const bool have = c < nc;
+        const int q = have ? cl[c] : 0;
+        const int tr = q / FT;
+        const int u0 = ty0 + tr, v0 = tx0 + (q - tr * FT);
+        int st = CAND_REJECT;
+        float y = 0.f, x = 0.f, m = 0.f;
+        unsigned int lp = 0, fp = 0;
+        if (have) {
             if (p.max_iter <= 0) {
                 st = CAND_PENDING;
             } else {
                 // walk_cols.wgsl:38-74
                 int u = u0, v = v0;
-                float c0 = 0.f, c1 = 0.f;
+                float w0 = 0.f, w1 = 0.f;
                 bool ok = true;
                 for (int iter = 0; iter < p.max_iter; ++iter) {
-                    if (!centroid_fixed<G, RC>(p, acc, u, v, c0, c1, m)) { ok = false; break; }
+                    if (!centroid_fixed<G, RC>(p, acc, u, v, w0, w1, m)) { ok = false; break; }
                     lp = ((unsigned)u << 16) | (unsigned)v;
                     bool changed = false;
-                    if (c0 > p.thr && u < H - 1) { u += 1; changed = true; }
-                    else if (c0 < -p.thr && u > 0) { u -= 1; changed = true; }
-                    if (c1 > p.thr && v < W - 1) { v += 1; changed = true; }
-                    else if (c1 < -p.thr && v > 0) { v -= 1; changed = true; }
+                    if (w0 > p.thr && u < H - 1) { u += 1; changed = true; }
+                    else if (w0 < -p.thr && u > 0) { u -= 1; changed = true; }
+                    if (w1 > p.thr && v < W - 1) { v += 1; changed = true; }
+                    else if (w1 < -p.thr && v > 0) { v -= 1; changed = true; }
                     if (!changed) break;
                 }
                 if (!ok) {
                     st = CAND_PENDING;
                     m = 0.f;
                 } else {
-                    y = (float)u + c0;
-                    x = (float)v + c1;
+                    y = (float)u + w0;
+                    x = (float)v + w1;
                     st = (m > p.minmass && m != 0.f) ? CAND_EMIT : CAND_REJECT;
                     fp = ((unsigned)u << 16) | (unsigned)v;
                 }
             }
-            wy[c] = y; wx[c] = x; wm[c] = m; wst[c] = st; wlp[c] = lp; wfp[c] = fp;
         }
-        __syncthreads();
-        const int cchunk = (nr + NTK - 1) / NTK;
-        const int c0 = tid * cchunk, c1 = min(c0 + cchunk, nr);
-        int ne = 0;
-        for (int c = c0; c < c1; ++c) ne += (wst[c] != CAND_REJECT);
-        int epos = block_excl_scan<NTK>(ne, warp_tot, &s_total);
-        const int nemit = s_total;
-        if (tid == 0) {
-            int base = 0;
-            if (nemit > 0) base = atomicAdd(b.fcount + t, nemit);
-            if (base + nemit > b.cap_c) { atomicOr(b.err, ERR_CAND_OVERFLOW); base = -1; }
-            s_base = base;
-        }
-        {
-            int e = emitted + epos;
-            for (int c = c0; c < c1; ++c) {
-                if (wst[c] == CAND_REJECT) continue;
-                const int tr = clist[r0 + c] / FT;
-                atomicMin(&rowstart[tr], e);
-                atomicAdd(&rowcount[tr], 1);
-                ++e;
+        const bool em = st != CAND_REJECT;
+        const unsigned eb = __ballot_sync(0xffffffffu, em);
+        int gbase = 0;
+        if (lane == 0 && eb) {
+            gbase = atomicAdd(b.fcount + t, __popc(eb));
+            if (gbase + __popc(eb) > b.cap_c) {
+                atomicOr(b.err, ERR_CAND_OVERFLOW);
+                gbase = -1;
             }
         }
-        __syncthreads();
-        const int base = s_base;
-        for (int c = c0; c < c1; ++c) {
-            if (wst[c] == CAND_REJECT) continue;
-            const int q = clist[r0 + c];
-            const int tr = q / FT;
-            const int u0 = ty0 + tr, v0 = tx0 + (q - tr * FT);
-            Cand rec;
+        const unsigned same = __match_any_sync(0xffffffffu, have ? tr : -1);
+        const int rowbase = have ? rowcount[tr] : 0;
+        const int rrank = __popc(eb & same & lt);
+        __syncwarp();
+        if (em && ((eb & same) >> lane) == 1u) rowcount[tr] = rowbase + rrank + 1;
+        Cand rec;
+        if (em) {
             rec.u = u0; rec.v = v0;
-            rec.y = wy[c]; rec.x = wx[c]; rec.mass = wm[c];
-            rec.rowrank = emitted + epos - rowstart[tr];
-            rec.state = wst[c];
+            rec.y = y; rec.x = x; rec.mass = m;
+            rec.rowrank = rowbase + rrank;
+            rec.state = st;
             rec.rg_sum = rec.eccn = rec.mid = rec.signal = 0.f;
             rec.g_rg = rec.g_raw = rec.g_sig = rec.g_ecc = 0.f;
-            rec.ul = (int)(wlp[c] >> 16); rec.vl = (int)(wlp[c] & 0xffffu);
-            rec.up = (int)(wfp[c] >> 16); rec.vp = (int)(wfp[c] & 0xffffu);
+            rec.ul = (int)(lp >> 16); rec.vl = (int)(lp & 0xffffu);
+            rec.up = (int)(fp >> 16); rec.vp = (int)(fp & 0xffffu);
             rec.pad = 0;
             if (p.cpu_processed) {
                 // execute_gpu.rs:165-172, 286-299 at the originating pixel
@@ -643,20 +629,24 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
                 rec.signal = sig;
             }
             if (p.characterize) gpu_features(p, b, acc, racc, u0, v0, rec);
-            if (base >= 0) {
-                const int slot = base + epos;
-                b.cand[(size_t)t * b.cap_c + slot] = rec;
-                if (rec.state == CAND_PENDING) {
-                    const int k = atomicAdd(b.npend, 1);
-                    b.pend[k] = t * b.cap_c + slot;
-                }
-            }
-            ++epos;
         }
-        emitted += nemit;
-        __syncthreads();
+        // the slot base is read only here, after the features: the atomic's
+        // round trip overlaps them
+        gbase = __shfl_sync(0xffffffffu, gbase, 0);
+        if (em && gbase >= 0) {
+            const int slot = gbase + __popc(eb & lt);
+            b.cand[(size_t)t * b.cap_c + slot] = rec;
+            if (rec.state == CAND_PENDING) {
+                const int k = atomicAdd(b.npend, 1);
+                b.pend[k] = t * b.cap_c + slot;
+            }
+        }
+        __syncwarp();
     }
-    for (int r = tid; r < TH; r += NTK) b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = rowcount[r];
+    if (lane < RPW) {
+        const int r = warp * RPW + lane;
+        if (r < TH) b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = rowcount[r];
+    }
 }
 
 // Checks div1() against IEEE division for 0 and every binary32 dividend in
