@@ -130,6 +130,27 @@ def test_raw_signal_even_annulus(gpu):
     check(mv, diameter=9, minmass=500, sig_radius=2.5, bg_radius=6.0)
 
 
+@pytest.mark.parametrize("rows", [64, 32])
+def test_candidate_flood_exact(gpu, rows):
+    """A checkerboard makes every other pixel an equal (non-strict) local
+    maximum: thousands of candidates per tile, more than the locate kernel
+    walks itself (the rest go to the fallback walk)."""
+    mv = np.full((2, 96, 160), 1000, np.uint16)
+    yy, xx = np.mgrid[0:96, 0:160]
+    board = np.where((yy + xx) % 2 == 0, 1200, 800).astype(np.uint16)
+    mv[0, 8:90, 4:150] = board[8:90, 4:150]
+    mv[1, 20:60, 70:140] = board[20:60, 70:140]
+    try:
+        _native.set_option("locate_tile_rows", rows)
+        tab, _ = check(mv, diameter=7, minmass=10.0, search_range=3.0, cpu_processed=True)
+        st = _native.last_stats()
+        assert st["locate_kernel"] == 2
+    finally:
+        _native.set_option("locate_tile_rows", 64)
+    assert st["candidates"] > 4000  # records before the separation filter
+    assert tab.shape[0] >= 10
+
+
 def test_blank_and_saturated_frames(gpu):
     mv = np.zeros((3, 64, 80), np.uint16)
     mv[1, 20:30, 30:40] = 65535     # saturated plateau: many equal maxima

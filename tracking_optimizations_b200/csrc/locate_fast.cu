@@ -19,10 +19,10 @@
 //      divides by the Gaussian norm and k^2, clips at 0 -> P2 (row pairs);
 //   4. row max over the dilation window (register sliding max) -> RM2;
 //   5. column max of RM2 compared with the centre -> local-max flags;
-//   6. each warp lists the flagged pixels of its own tile rows in raster
-//      order (ballots), walks them one per lane, computes the features and
-//      emits the records with one slot atomic per 32 candidates; warps do
-//      not wait for each other.
+//   6. the flagged pixels are listed by ballots and walked one per lane by
+//      as few warps as they need; those warps compute the features and
+//      emit the records (ranks from per-row bit masks, one slot atomic per
+//      warp).
 // Row strides of the pair arrays are odd (in 8-byte units), so every
 // lane-per-row access is bank-conflict free.
 #include <cuda.h>
@@ -285,8 +285,8 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     constexpr int HP = G::HP, HX = G::HX;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_fail;
-    __shared__ int rowcount[TH0];
+    __shared__ int s_fail, s_nc;
+    __shared__ unsigned long long rowmask[TH0];  // columns of the tile row that emit a record
 
     const int tid = threadIdx.x;
     const int tile = blockIdx.x;
@@ -341,7 +341,8 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         }
         __syncthreads();
     }
-    if (tid < TH0) rowcount[tid] = 0;
+    if (tid < TH0) rowmask[tid] = 0ull;
+    if (tid == 0) s_nc = 0;
     if (p.cpu_processed)
         for (int k = tid; k < G::K; k += NTK)
             sc[k] = make_float2(__ldg(b.char_tab + 3 * k + 1), __ldg(b.char_tab + 3 * k + 2));
@@ -522,130 +523,163 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     }
     __syncthreads();
 
-    // ---- 6. per-warp compaction, walks and emission ----
-    // Warp w owns tile rows [w * RPW, (w + 1) * RPW): its candidates are
-    // listed in raster order by ballots, walked one per lane, and emitted
-    // with slots from one atomic per round of 32, so no warp waits for
-    // another.  rowrank = rank among the emitted records of the (row, tile)
-    // segment, as finalize_kernel expects.
+    // ---- 6. candidate list, walks packed 32 per warp, emission ----
+    // Each warp appends the flagged pixels of its own tile rows to the CTA
+    // list; the list is then walked one candidate per lane by as few warps
+    // as it needs (the other warps leave), so the walks, which are the
+    // costliest code per candidate, run with full warps.  Records are ranked
+    // within their (row, tile) segment from a per-row bit mask of the
+    // columns that emit, which is what finalize_kernel needs; slots come
+    // from one atomic per warp.  Candidates beyond one per thread of the
+    // CTA are emitted as pending without a walk; fallback_walk_kernel walks
+    // them.
     constexpr int NW = NTK / 32;
     constexpr int RPW = TH0 / NW;
     static_assert(RPW * NW == TH0 && FT == 64, "warp row ownership");
     const int warp = tid >> 5, lane = tid & 31;
     const unsigned lt = (1u << lane) - 1u;
-    int* cl = clist + warp * (RPW * FT);
-    int nc = 0;
+    {
+        unsigned bals[2 * RPW];
+        int nc = 0;
 #pragma unroll
-    for (int rr = 0; rr < RPW; ++rr) {
-        const int r = warp * RPW + rr;
+        for (int k = 0; k < 2 * RPW; ++k) {
+            const int q = (warp * RPW + (k >> 1)) * FT + (k & 1) * 32 + lane;
+            bals[k] = __ballot_sync(0xffffffffu, flags[q] != 0);
+            nc += __popc(bals[k]);
+        }
+        int wbase = 0;
+        if (lane == 0 && nc) wbase = atomicAdd(&s_nc, nc);
+        wbase = __shfl_sync(0xffffffffu, wbase, 0);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int q = r * FT + h * 32 + lane;
-            const bool f = flags[q] != 0;
-            const unsigned bal = __ballot_sync(0xffffffffu, f);
-            if (f) cl[nc + __popc(bal & lt)] = q;
-            nc += __popc(bal);
+        for (int k = 0; k < 2 * RPW; ++k) {
+            if ((bals[k] >> lane) & 1u)
+                clist[wbase + __popc(bals[k] & lt)] = (warp * RPW + (k >> 1)) * FT + (k & 1) * 32 + lane;
+            wbase += __popc(bals[k]);
         }
     }
-    __syncwarp();
+    __syncthreads();
+    const int ncand = s_nc;
+    const int nwalk = min(NW, max(1, (ncand + 31) >> 5));
+    if (warp >= nwalk) return;  // only the named barrier below follows
+    const int wstride = nwalk * 32;
 
     P2Acc<G> acc{(const float*)P2, py0, px0};
+    const int c = warp * 32 + lane;
+    const bool have = c < ncand;
+    const int q = have ? clist[c] : 0;
+    const int tr = q / FT, tc = q - tr * FT;
+    const int u0 = ty0 + tr, v0 = tx0 + tc;
+    int st = CAND_REJECT;
+    float y = 0.f, x = 0.f, m = 0.f;
+    unsigned int lp = 0, fp = 0;
+    if (have) {
+        if (p.max_iter <= 0) {
+            st = CAND_PENDING;
+        } else {
+            // walk_cols.wgsl:38-74
+            int u = u0, v = v0;
+            float w0 = 0.f, w1 = 0.f;
+            bool ok = true;
+            for (int iter = 0; iter < p.max_iter; ++iter) {
+                if (!centroid_fixed<G, RC>(p, acc, u, v, w0, w1, m)) { ok = false; break; }
+                lp = ((unsigned)u << 16) | (unsigned)v;
+                bool changed = false;
+                if (w0 > p.thr && u < H - 1) { u += 1; changed = true; }
+                else if (w0 < -p.thr && u > 0) { u -= 1; changed = true; }
+                if (w1 > p.thr && v < W - 1) { v += 1; changed = true; }
+                else if (w1 < -p.thr && v > 0) { v -= 1; changed = true; }
+                if (!changed) break;
+            }
+            if (!ok) {
+                st = CAND_PENDING;
+                m = 0.f;
+            } else {
+                y = (float)u + w0;
+                x = (float)v + w1;
+                st = (m > p.minmass && m != 0.f) ? CAND_EMIT : CAND_REJECT;
+                fp = ((unsigned)u << 16) | (unsigned)v;
+            }
+        }
+    }
+    if (st != CAND_REJECT) atomicOr(&rowmask[tr], 1ull << tc);
+    int nrec = __popc(__ballot_sync(0xffffffffu, st != CAND_REJECT));
+    for (int c0 = wstride; c0 < ncand; c0 += wstride) {
+        const bool more = c0 + c < ncand;
+        if (more) {
+            const int q2 = clist[c0 + c];
+            atomicOr(&rowmask[q2 / FT], 1ull << (q2 % FT));
+        }
+        nrec += __popc(__ballot_sync(0xffffffffu, more));
+    }
+    int gbase = 0;
+    if (lane == 0 && nrec) {
+        gbase = atomicAdd(b.fcount + t, nrec);
+        if (gbase + nrec > b.cap_c) {
+            atomicOr(b.err, ERR_CAND_OVERFLOW);
+            gbase = -1;
+        }
+    }
+    if (nwalk > 1) asm volatile("bar.sync 1, %0;" ::"r"(wstride) : "memory");
+    else __syncwarp();
+    if (warp == 0)
+        for (int r = lane; r < TH; r += 32)
+            b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = __popcll(rowmask[r]);
+
+    // emission: round 0 from the walks above, later rounds pending
     const unsigned short* frame = (const unsigned short*)b.frames + (size_t)t * H * W;
     GRawAcc racc{frame, W};
-    for (int c0 = 0; c0 < nc; c0 += 32) {
-        const int c = c0 + lane;
-        const bool have = c < nc;
-        const int q = have ? cl[c] : 0;
-        const int tr = q / FT;
-        const int u0 = ty0 + tr, v0 = tx0 + (q - tr * FT);
-        int st = CAND_REJECT;
-        float y = 0.f, x = 0.f, m = 0.f;
-        unsigned int lp = 0, fp = 0;
-        if (have) {
-            if (p.max_iter <= 0) {
-                st = CAND_PENDING;
-            } else {
-                // walk_cols.wgsl:38-74
-                int u = u0, v = v0;
-                float w0 = 0.f, w1 = 0.f;
-                bool ok = true;
-                for (int iter = 0; iter < p.max_iter; ++iter) {
-                    if (!centroid_fixed<G, RC>(p, acc, u, v, w0, w1, m)) { ok = false; break; }
-                    lp = ((unsigned)u << 16) | (unsigned)v;
-                    bool changed = false;
-                    if (w0 > p.thr && u < H - 1) { u += 1; changed = true; }
-                    else if (w0 < -p.thr && u > 0) { u -= 1; changed = true; }
-                    if (w1 > p.thr && v < W - 1) { v += 1; changed = true; }
-                    else if (w1 < -p.thr && v > 0) { v -= 1; changed = true; }
-                    if (!changed) break;
-                }
-                if (!ok) {
-                    st = CAND_PENDING;
-                    m = 0.f;
-                } else {
-                    y = (float)u + w0;
-                    x = (float)v + w1;
-                    st = (m > p.minmass && m != 0.f) ? CAND_EMIT : CAND_REJECT;
-                    fp = ((unsigned)u << 16) | (unsigned)v;
-                }
-            }
+    gbase = __shfl_sync(0xffffffffu, gbase, 0);
+    int roff = 0;
+    for (int c0 = 0; c0 < ncand; c0 += wstride) {
+        int rq = q, rtr = tr, rtc = tc, rst = st;
+        float ry = y, rx = x, rm = m;
+        unsigned int rlp = lp, rfp = fp;
+        if (c0 > 0) {
+            const bool more = c0 + c < ncand;
+            rq = more ? clist[c0 + c] : 0;
+            rtr = rq / FT;
+            rtc = rq - rtr * FT;
+            rst = more ? CAND_PENDING : CAND_REJECT;
+            ry = rx = rm = 0.f;
+            rlp = rfp = 0;
         }
-        const bool em = st != CAND_REJECT;
+        const bool em = rst != CAND_REJECT;
         const unsigned eb = __ballot_sync(0xffffffffu, em);
-        int gbase = 0;
-        if (lane == 0 && eb) {
-            gbase = atomicAdd(b.fcount + t, __popc(eb));
-            if (gbase + __popc(eb) > b.cap_c) {
-                atomicOr(b.err, ERR_CAND_OVERFLOW);
-                gbase = -1;
-            }
-        }
-        const unsigned same = __match_any_sync(0xffffffffu, have ? tr : -1);
-        const int rowbase = have ? rowcount[tr] : 0;
-        const int rrank = __popc(eb & same & lt);
-        __syncwarp();
-        if (em && ((eb & same) >> lane) == 1u) rowcount[tr] = rowbase + rrank + 1;
-        Cand rec;
         if (em) {
-            rec.u = u0; rec.v = v0;
-            rec.y = y; rec.x = x; rec.mass = m;
-            rec.rowrank = rowbase + rrank;
-            rec.state = st;
+            const int ru = ty0 + rtr, rv = tx0 + rtc;
+            Cand rec;
+            rec.u = ru; rec.v = rv;
+            rec.y = ry; rec.x = rx; rec.mass = rm;
+            rec.rowrank = __popcll(rowmask[rtr] & ((1ull << rtc) - 1ull));
+            rec.state = rst;
             rec.rg_sum = rec.eccn = rec.mid = rec.signal = 0.f;
             rec.g_rg = rec.g_raw = rec.g_sig = rec.g_ecc = 0.f;
-            rec.ul = (int)(lp >> 16); rec.vl = (int)(lp & 0xffffu);
-            rec.up = (int)(fp >> 16); rec.vp = (int)(fp & 0xffffu);
+            rec.ul = (int)(rlp >> 16); rec.vl = (int)(rlp & 0xffffu);
+            rec.up = (int)(rfp >> 16); rec.vp = (int)(rfp & 0xffffu);
             rec.pad = 0;
             if (p.cpu_processed) {
                 // execute_gpu.rs:165-172, 286-299 at the originating pixel
-                const int rr = u0 - py0, cc = v0 - px0;
+                const int rr = ru - py0, cc = rv - px0;
                 const int base2 = (((rr >> 1) * G::P2S + cc) << 1);
                 float rg, sn, cs2, sig;
                 if (rr & 1) circle_features<RC, 1, G::P2S>((const float*)P2, base2, sc, rg, sn, cs2, sig);
                 else circle_features<RC, 0, G::P2S>((const float*)P2, base2, sc, rg, sn, cs2, sig);
                 rec.rg_sum = rg;
                 rec.eccn = sqrtf(sn * sn + cs2 * cs2);
-                rec.mid = acc(u0, v0);
+                rec.mid = acc(ru, rv);
                 rec.signal = sig;
             }
-            if (p.characterize) gpu_features(p, b, acc, racc, u0, v0, rec);
-        }
-        // the slot base is read only here, after the features: the atomic's
-        // round trip overlaps them
-        gbase = __shfl_sync(0xffffffffu, gbase, 0);
-        if (em && gbase >= 0) {
-            const int slot = gbase + __popc(eb & lt);
-            b.cand[(size_t)t * b.cap_c + slot] = rec;
-            if (rec.state == CAND_PENDING) {
-                const int k = atomicAdd(b.npend, 1);
-                b.pend[k] = t * b.cap_c + slot;
+            if (p.characterize) gpu_features(p, b, acc, racc, ru, rv, rec);
+            if (gbase >= 0) {
+                const int slot = gbase + roff + __popc(eb & lt);
+                b.cand[(size_t)t * b.cap_c + slot] = rec;
+                if (rec.state == CAND_PENDING) {
+                    const int k = atomicAdd(b.npend, 1);
+                    b.pend[k] = t * b.cap_c + slot;
+                }
             }
         }
-        __syncwarp();
-    }
-    if (lane < RPW) {
-        const int r = warp * RPW + lane;
-        if (r < TH) b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = rowcount[r];
+        roff += __popc(eb);
     }
 }
 
