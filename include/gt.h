@@ -226,6 +226,41 @@ GT_API int gt_ets_channels(const char* path, int32_t* channels, int32_t* frames,
 GT_API int gt_link(gt_ctx* ctx, const float* rows, int64_t n, int ncols, float search_range,
             int has_memory, uint32_t memory, uint64_t* ids);
 
+/* Trajectory post-processing of a linked table, the lab pipeline's steps
+ * after linking (all_cleaned_up/hatzakis_lab_tracking.py:216-230).  Host
+ * arrays of n rows in table order; `ids` is the particle column as
+ * integers.  Particles are taken in pandas' groupby order: ascending id,
+ * the rows of a particle in table order. */
+
+/* trackpy.filter_stubs(tracks, threshold) (hatzakis_lab_tracking.py:217):
+ * keep[i] = 1 when ids[i] occurs in at least `threshold` rows, else 0;
+ * *nkept = number of kept rows. */
+GT_API int gt_filter_stubs(gt_ctx* ctx, const int64_t* ids, int64_t n, int64_t threshold, uint8_t* keep,
+                           int64_t* nkept);
+
+/* step_tracker (hatzakis_lab_tracking.py:53-83): xs, ys = x * mpp, y * mpp
+ * (float32, table order); then per particle the step from its previous row
+ * (0 for its first row) and the step length sqrt(y_step^2 + x_step^2) in
+ * float64 (the lab code turns the float32 values into Python floats with
+ * tolist()).  x_step, y_step and steplength are in groupby order -- the
+ * sequence step_tracker assigns to the table by position -- and order[j] is
+ * the table row of entry j. */
+GT_API int gt_steps(gt_ctx* ctx, const int64_t* ids, const float* x, const float* y, int64_t n, double mpp,
+                    float* xs, float* ys, double* x_step, double* y_step, double* steplength, int64_t* order);
+
+/* Per-particle mean squared displacement, trackpy.msd(traj, mpp, fps,
+ * max_lagtime) of every particle concatenated and stacked as mp_imsd and
+ * tracker() do (hatzakis_lab_tracking.py:199-214, 230-232): positions
+ * xy * mpp (float32) on the frame axis from a particle's first to its last
+ * frame; for lag L = 1 .. min(max_lagtime, span - 1) the mean over pairs
+ * with both frames present of the squared x and y differences, summed.
+ * *out is an (m x 3) table (lag, particle, msd), ordered by lag then
+ * particle, without lags that have no pair; particle ids must lie in
+ * [0, 2^24).  A particle with two rows in one frame is GT_ERR_ARG (trackpy
+ * refuses it: one trajectory per particle).  Release with gt_table_free. */
+GT_API int gt_imsd(gt_ctx* ctx, const int64_t* ids, const int64_t* frames, const float* x, const float* y,
+                   int64_t n, double mpp, int64_t max_lagtime, gt_table* out);
+
 /* Locate (no linking) ONE device-resident frame while allocating nothing:
  * for callers that must not call cudaMalloc -- code running during CUDA
  * stream capture, processes whose device memory belongs to another
@@ -274,6 +309,7 @@ typedef struct gt_stats {
     float ms_adjoint_dense;     /* gt_adjoint_backward: zeroing + transposed bandpass */
     int32_t batch_graph;        /* gt_batch_many_device: 2 graph replayed, 1 graph built, 0 no graph */
     int32_t batch_fallbacks;    /* gt_batch_many_device: movies rerun through gt_batch_device */
+    float ms_msd;               /* gt_imsd: device time of the per-particle MSD kernel */
 } gt_stats;
 
 GT_API int gt_last_stats(const gt_ctx* ctx, gt_stats* out);

@@ -93,9 +93,10 @@ def test_struct_layouts_match_header(tmp_path):
 #include <stddef.h>
 #include "gt.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(gt_params), sizeof(gt_table), sizeof(gt_stats),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(gt_params), sizeof(gt_table), sizeof(gt_stats),
          offsetof(gt_params, gap_radius), offsetof(gt_table, names), offsetof(gt_stats, ms_total),
-         sizeof(gt_movie), offsetof(gt_movie, params), offsetof(gt_movie, out), offsetof(gt_stats, batch_fallbacks));
+         sizeof(gt_movie), offsetof(gt_movie, params), offsetof(gt_movie, out), offsetof(gt_stats, batch_fallbacks),
+         offsetof(gt_stats, ms_msd));
   return 0;
 }
 """)
@@ -105,7 +106,7 @@ int main(void) {
     want = [ctypes.sizeof(_native.GtParams), ctypes.sizeof(_native.GtTable), ctypes.sizeof(_native.GtStats),
             _native.GtParams.gap_radius.offset, _native.GtTable.names.offset, _native.GtStats.ms_total.offset,
             ctypes.sizeof(_native.GtMovie), _native.GtMovie.params.offset, _native.GtMovie.out.offset,
-            _native.GtStats.batch_fallbacks.offset]
+            _native.GtStats.batch_fallbacks.offset, _native.GtStats.ms_msd.offset]
     assert got == want
 
 

@@ -80,6 +80,7 @@ class GtStats(ctypes.Structure):
         ("ms_adjoint_dense", ctypes.c_float),
         ("batch_graph", ctypes.c_int32),
         ("batch_fallbacks", ctypes.c_int32),
+        ("ms_msd", ctypes.c_float),
     ]
 
 
@@ -109,6 +110,13 @@ SIGNATURES = [
     ("gt_batch_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.POINTER(GtParams), ctypes.c_void_p, ctypes.c_int64,
                                        ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]),
+    ("gt_filter_stubs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                        ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    ("gt_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_void_p]),
+    ("gt_imsd", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_int64, ctypes.c_double, ctypes.c_int64, ctypes.POINTER(GtTable)]),
     ("gt_link", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_float,
                                ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p]),
     ("gt_table_free", None, [ctypes.POINTER(GtTable)]),

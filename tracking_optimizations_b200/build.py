@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgt.so")
 SOURCES = ["gt_api.cu", "locate.cu", "locate_fast.cu", "finalize.cu", "link.cu", "assemble.cu", "noalloc.cu",
-           "adjoint.cu", "synth.cu", "ingest.cpp"]
+           "adjoint.cu", "synth.cu", "traj.cu", "ingest.cpp"]
 
 # --fmad=false: the only fused multiply-adds are explicit fmaf() calls, so the
 # kernels reproduce the oracle's operation order bit for bit.

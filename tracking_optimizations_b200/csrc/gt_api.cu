@@ -50,6 +50,14 @@ cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* 
 cudaError_t launch_adjoint_transpose(const AdjParams& p, const float* gR, float* gI, cudaStream_t st);
 __global__ void link_fixpoint_multi_kernel(const LinkBufs* Ls, const int* memory, const int* fstart, int nm,
                                            int max_passes, int* ndirty, int* passes);
+int traj_filter_stubs(const int64_t* h_ids, int64_t n, int64_t threshold, uint8_t* h_keep, int64_t* nkept,
+                      cudaStream_t st, int num_sms, std::string* msg);
+int traj_steps(const int64_t* h_ids, const float* h_x, const float* h_y, int64_t n, float mppf, float* h_xs,
+               float* h_ys, double* h_xstep, double* h_ystep, double* h_len, int64_t* h_order, cudaStream_t st,
+               int num_sms, std::string* msg);
+int traj_imsd(const int64_t* h_ids, const int64_t* h_frames, const float* h_x, const float* h_y, int64_t n,
+              float mppf, int64_t max_lagtime, float* (*alloc)(size_t), float** out, int64_t* nout, float* ms_msd,
+              cudaStream_t st, int num_sms, std::string* msg);
 }  // namespace gt
 
 using namespace gt;
@@ -1848,6 +1856,81 @@ int gt_ctx_set_option(gt_ctx* ctx, const char* key, int value) {
 
 void gt_table_free(gt_table* table) {
     if (table && table->data) { table_release(table->data); table->data = nullptr; }
+}
+
+namespace {
+// trajectory entry points share the argument checks
+int traj_begin(gt_ctx* ctx, int64_t n, bool ok_ptrs) {
+    if (!ctx) return GT_ERR_ARG;
+    ctx->err.clear();
+    ctx->stats = gt_stats{};
+    if (n < 0 || (n > 0 && !ok_ptrs)) {
+        ctx->err = "invalid arrays";
+        return GT_ERR_ARG;
+    }
+    if (n >= ((int64_t)1 << 31)) {
+        ctx->err = "table too large";
+        return GT_ERR_ARG;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        ctx->err = "cudaSetDevice failed";
+        return GT_ERR_CUDA;
+    }
+    return GT_OK;
+}
+}  // namespace
+
+int gt_filter_stubs(gt_ctx* ctx, const int64_t* ids, int64_t n, int64_t threshold, uint8_t* keep, int64_t* nkept) {
+    int rc = traj_begin(ctx, n, ids && keep && nkept);
+    if (rc || !nkept) return rc ? rc : GT_ERR_ARG;
+    *nkept = 0;
+    if (n == 0) return GT_OK;
+    return traj_filter_stubs(ids, n, threshold, keep, nkept, ctx->stream, ctx->num_sms, &ctx->err);
+}
+
+int gt_steps(gt_ctx* ctx, const int64_t* ids, const float* x, const float* y, int64_t n, double mpp, float* xs,
+             float* ys, double* x_step, double* y_step, double* steplength, int64_t* order) {
+    int rc = traj_begin(ctx, n, ids && x && y && xs && ys && x_step && y_step && steplength && order);
+    if (rc) return rc;
+    if (n == 0) return GT_OK;
+    return traj_steps(ids, x, y, n, (float)mpp, xs, ys, x_step, y_step, steplength, order, ctx->stream,
+                      ctx->num_sms, &ctx->err);
+}
+
+int gt_imsd(gt_ctx* ctx, const int64_t* ids, const int64_t* frames, const float* x, const float* y, int64_t n,
+            double mpp, int64_t max_lagtime, gt_table* out) {
+    if (!out) return GT_ERR_ARG;
+    out->data = nullptr;
+    out->nrows = 0;
+    out->ncols = 0;
+    int rc = traj_begin(ctx, n, ids && frames && x && y);
+    if (rc) return rc;
+    float* data = nullptr;
+    int64_t m = 0;
+    float ms = 0.f;
+    if (n > 0) {
+        rc = traj_imsd(ids, frames, x, y, n, (float)mpp, max_lagtime, table_alloc, &data, &m, &ms, ctx->stream,
+                       ctx->num_sms, &ctx->err);
+        if (rc) {
+            if (data) table_release(data);
+            return rc;
+        }
+    } else {
+        data = table_alloc(sizeof(float) * 3);
+        if (!data) { ctx->err = "host allocation failed"; return GT_ERR_OOM; }
+    }
+    ctx->stats.ms_msd = ms;
+    out->data = data;
+    out->nrows = m;
+    out->ncols = 3;
+    std::memset(out->names, 0, sizeof(out->names));
+    std::memset(out->types, 0, sizeof(out->types));
+    const char* names[3] = {"lag", "particle", "msd"};
+    for (int i = 0; i < 3; ++i) {
+        std::snprintf(out->names[i], sizeof(out->names[i]), "%s", names[i]);
+        std::snprintf(out->types[i], sizeof(out->types[i]), "%s", i < 2 ? "int" : "float");
+    }
+    return GT_OK;
 }
 
 int gt_last_stats(const gt_ctx* ctx, gt_stats* out) {
