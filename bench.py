@@ -481,6 +481,86 @@ def run_file(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def run_postprocess(args, rank, world, local):
+    """--workload postprocess: the lab pipeline's steps after linking
+    (all_cleaned_up/hatzakis_lab_tracking.py:216-232: filter_stubs,
+    step_tracker, durations, per-particle MSD with max_lagtime = the longest
+    duration) on the linked table of the throughput movie, through
+    trajectories.postprocess (host DataFrame in, DataFrames out: uploads,
+    kernels and downloads inside the timed region).  Lab defaults:
+    duration_filter 20, pixel_size 0.18333, tracking_time 0.036.  Particles
+    that the reference's memory dedupe gave two rows in one frame are dropped
+    first (trackpy's msd refuses them)."""
+    import pandas as pd
+    import torch
+
+    from tracking_optimizations_b200 import _native, batch_rust, synth, trajectories
+
+    torch.cuda.set_device(local)
+    spec, params = workload()
+    rspec = synth.scaled(spec, frames=args.frames or spec.frames, seed=spec.seed + rank)
+    tab, cols = batch_rust(synth.make_movie(rspec), device=local, **params)
+    names = [c[0] for c in cols]
+    df = pd.DataFrame({k: tab[:, names.index(k)] for k in ("frame", "y", "x", "particle")})
+    ids = df["particle"].to_numpy().astype(np.int64)
+    key = ids * 1000003 + df["frame"].to_numpy().astype(np.int64)
+    _, inv, cnt = np.unique(key, return_inverse=True, return_counts=True)
+    branching = np.unique(ids[cnt[inv] > 1])
+    df = df[~np.isin(ids, branching)].reset_index(drop=True)
+
+    class Params:
+        duration_filter = 20
+        pixel_size = 0.18333
+        tracking_time = 0.036
+
+    for _ in range(max(3, args.warmup)):
+        full, msd_df = trajectories.postprocess(df, Params)
+    ms_msd = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        full, msd_df = trajectories.postprocess(df, Params)
+        ms_msd.append(_native.last_stats(local)["ms_msd"])
+    dt = (time.perf_counter() - t0) / args.steps
+    dt_max = max_over_ranks(dt, world, f"cuda:{local}")
+    if rank != 0:
+        return
+    n = len(df)
+    line = {
+        "metric": "linked-table rows/s through the lab post-processing (filter_stubs, step_tracker, imsd)",
+        "value": aggregate_rate(n, world, dt_max * 1e3), "unit": "rows/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": dt_max * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 positions / f64 sums",
+        "data": "synthetic: the linked table of the throughput movie",
+        "config": dict(config_dict(spec, params, world), workload=f"post-processing of {n} linked rows "
+                       f"({len(branching)} branching particles dropped): duration_filter 20, pixel_size 0.18333, "
+                       "tracking_time 0.036"),
+        "rows_kept": int(len(full)), "particles": int(full["particle"].nunique()),
+        "msd_entries": int(len(msd_df)), "max_lagtime": int(full["duration"].max()),
+        "msd_kernel_ms": float(np.median(ms_msd)),
+        "e2e": {"value": aggregate_rate(n, world, dt_max * 1e3), "unit": "rows/s",
+                "h2d_bytes_per_step": int(len(df) * (8 + 4 + 4) * 3),
+                "d2h_bytes_per_step": int(len(df) * (1 + 4 * 2 + 8 * 4) + len(msd_df) * 12),
+                "timing": "host clock around trajectories.postprocess"},
+    }
+    if not args.no_cpu_baseline:
+        from oracle import traj_ref
+        ids_k = full["particle"].to_numpy()
+        pids = np.unique(ids_k)
+        t0 = time.perf_counter()
+        done = 0
+        for i in range(0, len(pids), 64):
+            sel = np.isin(ids_k, pids[i:i + 64])
+            traj_ref.imsd(ids_k[sel], full["frame"].to_numpy()[sel], full["x"].to_numpy()[sel],
+                          full["y"].to_numpy()[sel], Params.pixel_size, int(full["duration"].max()))
+            done += int(sel.sum())
+            if time.perf_counter() - t0 > 12.0:
+                break
+        cdt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": done / cdt, "unit": "rows/s", "cores": 1, "kind": "port",
+                                "sample": f"MSD of the first {done} kept rows (numpy restatement, one core)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -489,7 +569,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="locate-link", choices=["locate-link", "adjoint", "batched", "file"])
+    ap.add_argument("--workload", default="locate-link", choices=["locate-link", "adjoint", "batched", "file",
+                                                                     "postprocess"])
     ap.add_argument("--frames", type=int, default=None,
                     help="smaller movie of the same spot model (profiling captures only)")
     args = ap.parse_args()
@@ -507,6 +588,9 @@ def main():
         return
     if args.workload == "file":
         run_file(args, rank, world, local)
+        return
+    if args.workload == "postprocess":
+        run_postprocess(args, rank, world, local)
         return
 
     import torch

@@ -234,9 +234,11 @@ GT_API int gt_link(gt_ctx* ctx, const float* rows, int64_t n, int ncols, float s
 
 /* trackpy.filter_stubs(tracks, threshold) (hatzakis_lab_tracking.py:217):
  * keep[i] = 1 when ids[i] occurs in at least `threshold` rows, else 0;
- * *nkept = number of kept rows. */
+ * *nkept = number of kept rows.  count (may be NULL) receives the number of
+ * rows of each row's particle -- the duration column of line 223 for the
+ * kept rows. */
 GT_API int gt_filter_stubs(gt_ctx* ctx, const int64_t* ids, int64_t n, int64_t threshold, uint8_t* keep,
-                           int64_t* nkept);
+                           int64_t* count, int64_t* nkept);
 
 /* step_tracker (hatzakis_lab_tracking.py:53-83): xs, ys = x * mpp, y * mpp
  * (float32, table order); then per particle the step from its previous row

@@ -48,6 +48,8 @@ def test_filter_stubs_steps_imsd_on_a_linked_table(gpu):
     ids = t["particle"].astype(np.int64)
     for thr in [0, 1, 5, 20, 41]:
         np.testing.assert_array_equal(trajectories.filter_stubs(ids, thr), traj_ref.filter_stubs(ids, thr))
+    _, inv, cnt = np.unique(ids, return_inverse=True, return_counts=True)
+    np.testing.assert_array_equal(trajectories.filter_stubs(ids, 3, return_counts=True)[1], cnt[inv])
     keep = traj_ref.filter_stubs(ids, 10)
     ids_k, f_k, x_k, y_k = ids[keep], t["frame"][keep].astype(np.int64), t["x"][keep], t["y"][keep]
     got = trajectories.steps(ids_k, x_k, y_k, 0.18333)

@@ -111,7 +111,7 @@ SIGNATURES = [
                                        ctypes.c_int, ctypes.POINTER(GtParams), ctypes.c_void_p, ctypes.c_int64,
                                        ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]),
     ("gt_filter_stubs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
-                                        ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     ("gt_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                 ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                 ctypes.c_void_p, ctypes.c_void_p]),

@@ -50,8 +50,8 @@ cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* 
 cudaError_t launch_adjoint_transpose(const AdjParams& p, const float* gR, float* gI, cudaStream_t st);
 __global__ void link_fixpoint_multi_kernel(const LinkBufs* Ls, const int* memory, const int* fstart, int nm,
                                            int max_passes, int* ndirty, int* passes);
-int traj_filter_stubs(const int64_t* h_ids, int64_t n, int64_t threshold, uint8_t* h_keep, int64_t* nkept,
-                      cudaStream_t st, int num_sms, std::string* msg);
+int traj_filter_stubs(const int64_t* h_ids, int64_t n, int64_t threshold, uint8_t* h_keep, int64_t* h_count,
+                      int64_t* nkept, cudaStream_t st, int num_sms, std::string* msg);
 int traj_steps(const int64_t* h_ids, const float* h_x, const float* h_y, int64_t n, float mppf, float* h_xs,
                float* h_ys, double* h_xstep, double* h_ystep, double* h_len, int64_t* h_order, cudaStream_t st,
                int num_sms, std::string* msg);
@@ -1880,12 +1880,13 @@ int traj_begin(gt_ctx* ctx, int64_t n, bool ok_ptrs) {
 }
 }  // namespace
 
-int gt_filter_stubs(gt_ctx* ctx, const int64_t* ids, int64_t n, int64_t threshold, uint8_t* keep, int64_t* nkept) {
+int gt_filter_stubs(gt_ctx* ctx, const int64_t* ids, int64_t n, int64_t threshold, uint8_t* keep, int64_t* count,
+                    int64_t* nkept) {
     int rc = traj_begin(ctx, n, ids && keep && nkept);
     if (rc || !nkept) return rc ? rc : GT_ERR_ARG;
     *nkept = 0;
     if (n == 0) return GT_OK;
-    return traj_filter_stubs(ids, n, threshold, keep, nkept, ctx->stream, ctx->num_sms, &ctx->err);
+    return traj_filter_stubs(ids, n, threshold, keep, count, nkept, ctx->stream, ctx->num_sms, &ctx->err);
 }
 
 int gt_steps(gt_ctx* ctx, const int64_t* ids, const float* x, const float* y, int64_t n, double mpp, float* xs,

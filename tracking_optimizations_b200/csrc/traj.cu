@@ -69,14 +69,18 @@ __global__ void gstart_kernel(const unsigned long long* keys, int64_t n, const i
         if (j == 0 || gkey(keys[j - 1]) != gkey(keys[j])) gstart[gid[j]] = j;
 }
 
-// keep[row] for every row of groups with at least `threshold` rows
+// keep[row] for every row of groups with at least `threshold` rows;
+// count[row] = rows of the row's group
 __global__ void stubs_kernel(const unsigned long long* keys, int64_t n, const int64_t* gstart, int64_t G,
-                             int64_t threshold, uint8_t* keep, unsigned long long* nkept) {
+                             int64_t threshold, uint8_t* keep, int64_t* count, unsigned long long* nkept) {
     unsigned long long mine = 0;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G; g += (int64_t)gridDim.x * blockDim.x) {
         const int64_t j = gstart[g], e = g + 1 < G ? gstart[g + 1] : n;
         const uint8_t k = (e - j) >= threshold ? 1 : 0;
-        for (int64_t q = j; q < e; ++q) keep[keys[q] & 0xffffffffu] = k;
+        for (int64_t q = j; q < e; ++q) {
+            keep[keys[q] & 0xffffffffu] = k;
+            count[keys[q] & 0xffffffffu] = e - j;
+        }
         if (k) mine += (unsigned long long)(e - j);
     }
     if (mine) atomicAdd(nkept, mine);
@@ -319,21 +323,23 @@ int exclusive_sum(const int64_t* v, int64_t* o, int64_t G, DevBuf& B, cudaStream
 
 }  // namespace
 
-int traj_filter_stubs(const int64_t* h_ids, int64_t n, int64_t threshold, uint8_t* h_keep, int64_t* nkept,
-                      cudaStream_t st, int num_sms, std::string* msg) {
+int traj_filter_stubs(const int64_t* h_ids, int64_t n, int64_t threshold, uint8_t* h_keep, int64_t* h_count,
+                      int64_t* nkept, cudaStream_t st, int num_sms, std::string* msg) {
     DevBuf B(st);
     const int grid = num_sms * 8;
     Groups Gr;
     int rc = make_groups(h_ids, n, B, st, grid, &Gr, msg);
     if (rc) return rc;
     uint8_t* keep = B.get<uint8_t>(n);
+    int64_t* count = B.get<int64_t>(n);
     unsigned long long* cnt = B.get<unsigned long long>(1);
-    TA(keep && cnt);
+    TA(keep && count && cnt);
     TK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
-    stubs_kernel<<<grid, 256, 0, st>>>(Gr.keys, n, Gr.gstart, Gr.G, threshold, keep, cnt);
+    stubs_kernel<<<grid, 256, 0, st>>>(Gr.keys, n, Gr.gstart, Gr.G, threshold, keep, count, cnt);
     TK(cudaGetLastError());
     unsigned long long hk = 0;
     TK(cudaMemcpyAsync(h_keep, keep, n, cudaMemcpyDeviceToHost, st));
+    if (h_count) TK(cudaMemcpyAsync(h_count, count, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, st));
     TK(cudaMemcpyAsync(&hk, cnt, sizeof(hk), cudaMemcpyDeviceToHost, st));
     TK(cudaStreamSynchronize(st));
     *nkept = (int64_t)hk;

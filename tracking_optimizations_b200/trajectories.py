@@ -38,17 +38,20 @@ def _ids(a):
     return _i64(a)
 
 
-def filter_stubs(ids, threshold=100, device=0):
+def filter_stubs(ids, threshold=100, device=0, return_counts=False):
     """Boolean mask of the rows whose particle occurs in at least
-    ``threshold`` rows (trackpy.filter_stubs as the lab pipeline calls it)."""
+    ``threshold`` rows (trackpy.filter_stubs as the lab pipeline calls it);
+    with ``return_counts`` also the number of rows of each row's particle."""
     ids = _ids(ids)
     n = len(ids)
     keep = np.zeros(n, np.uint8)
+    count = np.zeros(n, np.int64)
     nk = ctypes.c_int64()
     lib = _native.load()
     ctx = _native.context(device)
-    _native.check(lib.gt_filter_stubs(ctx, _ptr(ids), n, int(threshold), _ptr(keep), ctypes.byref(nk)), ctx)
-    return keep.view(bool)
+    _native.check(lib.gt_filter_stubs(ctx, _ptr(ids), n, int(threshold), _ptr(keep), _ptr(count),
+                                      ctypes.byref(nk)), ctx)
+    return (keep.view(bool), count) if return_counts else keep.view(bool)
 
 
 def steps(ids, x, y, mpp, device=0):
@@ -119,12 +122,17 @@ def postprocess(df, params):
     ``(full_tracked, msd_df)`` with msd_df's columns time, particle, msd."""
     import pandas as pd
 
-    keep = filter_stubs(df["particle"].to_numpy(), params.duration_filter)
-    full = df[keep].copy()
-    full = step_tracker(full, params)
-    full["particle"] = full["particle"].transform(int)
-    full["duration"] = full.groupby("particle")["particle"].transform(len)
-    maxlag = int(full["duration"].max()) if len(full) else 0
-    t, p, m = imsd(full["particle"].to_numpy(), full["frame"].to_numpy(), full["x"].to_numpy(),
-                   full["y"].to_numpy(), params.pixel_size, float(params.tracking_time), max_lagtime=maxlag)
+    ids = _ids(df["particle"].to_numpy())
+    keep, count = filter_stubs(ids, params.duration_filter, return_counts=True)
+    cols = {c: df[c].to_numpy()[keep] for c in df.columns}
+    ids = ids[keep]
+    xs, ys, xst, yst, ln, _ = steps(ids, cols["x"], cols["y"], params.pixel_size)
+    cols["x"], cols["y"] = xs, ys
+    # step_tracker's columns (by position), the integer particle ids of
+    # transform(int) and groupby(...).transform(len) -- a particle's rows
+    # are all kept or all dropped, so its count is its duration
+    cols.update(x_step=xst, y_step=yst, steplength=ln, particle=ids, duration=count[keep])
+    full = pd.DataFrame(cols, index=df.index[keep])
+    maxlag = int(cols["duration"].max()) if len(ids) else 0
+    t, p, m = imsd(ids, cols["frame"], xs, ys, params.pixel_size, float(params.tracking_time), max_lagtime=maxlag)
     return full, pd.DataFrame({"time": t, "particle": p, "msd": m})
