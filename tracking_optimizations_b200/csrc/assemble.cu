@@ -31,6 +31,27 @@ __global__ void __launch_bounds__(1024) scan_frames_kernel(const int* in, int* o
     if (threadIdx.x == 0) out[n] = carry;
 }
 
+// Continues the exclusive scan of in[] into out[] over [f0, f0 + n): out[f0]
+// holds the prefix of the earlier frames (0 when f0 = 0); writes
+// out[f0 + 1 .. f0 + n].
+__global__ void __launch_bounds__(1024) scan_frames_from_kernel(const int* in, int* out, int f0, int n) {
+    __shared__ int warp_tot[32];
+    __shared__ int s_total;
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = f0 > 0 ? out[f0] : 0;
+    __syncthreads();
+    for (int b0 = 0; b0 < n; b0 += 1024) {
+        const int i = b0 + threadIdx.x;
+        const int v = i < n ? in[f0 + i] : 0;
+        const int e = block_excl_scan<1024>(v, warp_tot, &s_total);
+        if (i < n) out[f0 + i] = carry + e;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += s_total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[f0 + n] = carry;
+}
+
 // newid[g] for particles that start a trajectory: running counter in
 // (frame, index) order (linking.rs:470).
 __global__ void newid_kernel(const int* newrank, const int* newbase, const int* off, const int* npart,

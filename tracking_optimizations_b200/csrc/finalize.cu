@@ -76,11 +76,11 @@ __device__ __forceinline__ bool within_r(float qy, float qx, float iy, float ix,
 }  // namespace
 
 __global__ void __launch_bounds__(NTF) finalize_kernel(const LocParams p, MovieBufs b, float sep,
-                                                       int link_grid) {
+                                                       int link_grid, int frame0) {
     __shared__ int warp_tot[NTF / 32];
     __shared__ int s_total;
     extern __shared__ int cnt_s[];  // ncell ints (<= MAX_CELLS)
-    const int t = blockIdx.x;
+    const int t = frame0 + blockIdx.x;
     const int cap_c = b.cap_c;
     const int nrc = p.H * p.ntx;
     int* rc = b.rowcnt + (size_t)t * nrc;

@@ -28,11 +28,12 @@
 
 namespace gt {
 __global__ void locate_tiles_kernel(const LocParams p, const MovieBufs b, int frame0);
-__global__ void fallback_walk_kernel(const LocParams p, const MovieBufs b, int win);
-__global__ void finalize_kernel(const LocParams p, MovieBufs b, float sep, int link_grid);
+__global__ void fallback_walk_kernel(const LocParams p, const MovieBufs b, int win, const int* pbeg);
+__global__ void finalize_kernel(const LocParams p, MovieBufs b, float sep, int link_grid, int frame0);
 __global__ void link_fixpoint_kernel(LinkBufs L, int memory, int max_passes, int rounds, int* ndirty,
                                      int* passes, unsigned long long* phase_ns);
 __global__ void scan_frames_kernel(const int* in, int* out, int n);
+__global__ void scan_frames_from_kernel(const int* in, int* out, int f0, int n);
 __global__ void newid_kernel(const int* newrank, const int* newbase, const int* off, const int* npart,
                              int* newid, int T);
 __global__ void assemble_kernel(AsmArgs a);
@@ -102,6 +103,7 @@ constexpr long long SUBNET_BUDGET = 1LL << 26;  // option trials per subnet
 // that one round of blocks covers ~600 frames; frames whose data does not
 // fit use the block's global scratch slot
 constexpr int LINK_POOL_BYTES = 48 * 1024;
+constexpr int LINK_WINDOWS = 16;  // upload chunks of the host-frames path, at most
 
 struct Resolved {
     // lib.rs:77-91 defaults
@@ -359,6 +361,7 @@ struct Work {
     int *char_off, *sig_off, *bg_off;
     int* err;
     int *off, *pred, *mlist, *mcount, *dirty, *ndirty, *newrank, *newcount, *newbase, *root, *newid;
+    int* pbeg;  // fallback list position at the start of each chunk's locate
     unsigned long long* phase_ns;
     unsigned char* lnext;
     float *s_y, *s_x, *e_w, *d_w;
@@ -418,7 +421,8 @@ size_t carve(const Plan& P, char* base, Work* w, size_t frame_bytes, bool need_l
     w->mlist = c.take<int>(P.link ? T * P.cap_m : 1);
     w->mcount = c.take<int>(T);
     w->dirty = c.take<int>(T);
-    w->ndirty = c.take<int>(T + 2);
+    w->ndirty = c.take<int>((T + 2) * LINK_WINDOWS);  // per linker launch (frame window)
+    w->pbeg = c.take<int>(LINK_WINDOWS);
     w->phase_ns = c.take<unsigned long long>(4);
     w->newrank = c.take<int>(np);
     w->newcount = c.take<int>(T);
@@ -469,6 +473,8 @@ int ensure_arena(gt_ctx* ctx, size_t bytes) {
 
 LinkBufs link_bufs(const Plan& P, const Work& w) {
     LinkBufs L{};
+    L.tb = 0;
+    L.te = P.T;
     L.T = P.T; L.cap_p = P.cap_p; L.cap_m = P.cap_m; L.cap_e = P.cap_e; L.cap_s = P.cap_s;
     L.r = P.r.search_range;
     L.G = P.G; L.ncx = P.ncx; L.ncy = P.ncy;
@@ -487,36 +493,62 @@ LinkBufs link_bufs(const Plan& P, const Work& w) {
 }
 
 // Linking over the particle tables already in the workspace (npart, py, px,
-// gstart/gidx, off): one cooperative launch runs the whole fixed point
-// (link_fixpoint_kernel), then new trajectory ids are numbered.  Leaves the
-// trajectory id of particle g in newid[root[g]].
-int run_link(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
-    LinkBufs L = link_bufs(P, w);
-    int T = P.T;
+// gstart/gidx, off): cooperative launches of link_fixpoint_kernel run the
+// fixed point, then new trajectory ids are numbered.  Leaves the trajectory
+// id of particle g in newid[root[g]].
+//
+// The linker in frame windows.  link_window links frames [tb, te) to their
+// fixed point, given final links for the frames before tb: the memory
+// entries of a frame depend only on earlier frames, so windows taken in
+// order give the sequential result (the host-frames path links each
+// uploaded chunk while the next one is copied).  link_prepare runs once
+// before the first window, link_finish once after the last.
+int link_prepare(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
+    const int T = P.T;
     CK(cudaMemsetAsync(w.mcount, 0, sizeof(int) * T, st));
     CK(cudaMemsetAsync(w.dirty, 0, sizeof(int) * T, st));
-    CK(cudaMemsetAsync(w.ndirty, 0, sizeof(int) * (T + 2), st));
-    int rounds = 1;
-    while ((1 << rounds) < T + 1) ++rounds;
-    rounds += 1;
+    CK(cudaMemsetAsync(w.ndirty, 0, sizeof(int) * (T + 2) * LINK_WINDOWS, st));
+    CK(cudaMemsetAsync(w.phase_ns, 0, sizeof(unsigned long long) * 4, st));
+    return GT_OK;
+}
+
+int link_window(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st, int tb, int te, int wi) {
+    LinkBufs L = link_bufs(P, w);
+    L.tb = tb;
+    L.te = te;
+    const int T = P.T;
+    int rounds = 0;
     L.lsm_bytes = LINK_POOL_BYTES;
     CK(cudaFuncSetAttribute(link_fixpoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.lsm_bytes));
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_kernel, 256, L.lsm_bytes));
     const int grid = std::max(1, std::min(P.nslot, per_sm * ctx->num_sms));
     int memory = (int)P.r.memory;
-    int max_passes = T + 1;
-    int* ndirty = w.ndirty;
+    int max_passes = te - tb + 1;
+    int* ndirty = w.ndirty + (size_t)wi * (T + 2);
     int* passes = w.err + 1;
     unsigned long long* phase_ns = w.phase_ns;
     void* args[] = {&L, &memory, &max_passes, &rounds, &ndirty, &passes, &phase_ns};
     CK(cudaLaunchCooperativeKernel((const void*)link_fixpoint_kernel, dim3(grid), dim3(256), args, L.lsm_bytes,
                                    st));
+    ctx->stats.launches += 1;
+    return GT_OK;
+}
+
+int link_finish(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
+    const int T = P.T;
     scan_frames_kernel<<<1, 1024, 0, st>>>(w.newcount, w.newbase, T);
     newid_kernel<<<T, 256, 0, st>>>(w.newrank, w.newbase, w.off, w.npart, w.newid, T);
     CK(cudaGetLastError());
-    ctx->stats.launches += 3;
+    ctx->stats.launches += 2;
     return GT_OK;
+}
+
+int run_link(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
+    int rc = link_prepare(ctx, P, w, st);
+    if (!rc) rc = link_window(ctx, P, w, st, 0, P.T, 0);
+    if (!rc) rc = link_finish(ctx, P, w, st);
+    return rc;
 }
 
 int upload_tables(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
@@ -634,17 +666,51 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
         ++ci;
         return GT_OK;
     };
+    // With host frames and linking, each uploaded chunk is also finalized
+    // (pending walks, ordering, separation filter, offsets) and linked
+    // behind its copy, so only the last chunk's work follows the upload.
+    const int nchunks = (T + chunk - 1) / chunk;
+    const bool chunked = h_frames && P.link && nchunks > 1 && nchunks <= LINK_WINDOWS;
+    if (P.link) {
+        rc = link_prepare(ctx, P, w, st);
+        if (rc) return rc;
+    }
+    CK(cudaMemsetAsync(w.pbeg, 0, sizeof(int) * LINK_WINDOWS, st));
+    CK(cudaFuncSetAttribute(fallback_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_fb));
+    CK(cudaFuncSetAttribute(finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_fin));
+    int wi = 0;
+    auto post = [&](int f0, int nf) -> int {
+        fallback_walk_kernel<<<ctx->num_sms * 4, 128, P.smem_fb, st>>>(P.lp, b, P.fb_win, w.pbeg + wi);
+        finalize_kernel<<<nf, 512, P.smem_fin, st>>>(P.lp, b, P.sep, P.link, f0);
+        scan_frames_from_kernel<<<1, 1024, 0, st>>>(w.npart, w.off, f0, nf);
+        CK(cudaGetLastError());
+        ctx->stats.launches += 3;
+        if (P.link) {
+            const int r2 = link_window(ctx, P, w, st, f0, f0 + nf, wi);
+            if (r2) return r2;
+        }
+        ++wi;
+        return GT_OK;
+    };
+    // the fallback list position where chunk wi's entries begin
+    auto mark = [&]() -> int {
+        if (chunked && wi > 0) CK(cudaMemcpyAsync(w.pbeg + wi, w.npend, sizeof(int), cudaMemcpyDeviceToDevice, st));
+        return GT_OK;
+    };
     if (fast) {
         CK(cudaEventRecord(ctx->ev[0], st));
         for (int f0 = 0; f0 < T; f0 += chunk) {
-            rc = stage(f0, std::min(chunk, T - f0));
+            const int nf = std::min(chunk, T - f0);
+            rc = stage(f0, nf);
+            if (!rc) rc = mark();
             if (rc) return rc;
-            dim3 grid(ntiles, std::min(chunk, T - f0));
+            dim3 grid(ntiles, nf);
             int used_tma = 0;
             CK(launch_locate_fast(P.lp.krad, P.lp.D, P.lp.rint_c, P.fast_th, grid, st, P.lp, b, dn, dk, T, f0,
                                   &used_tma));
             ctx->stats.launches += 1;
             ctx->stats.locate_kernel = used_tma ? 2 : 1;
+            if (chunked && (rc = post(f0, nf))) return rc;
         }
     } else {
         LocParams lg = P.lp;  // generic tile plan (its own tile height)
@@ -654,27 +720,30 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
         lg.nty = (P.H + LOC_TH - 1) / LOC_TH;
         CK(cudaEventRecord(ctx->ev[0], st));
         for (int f0 = 0; f0 < T; f0 += chunk) {
-            rc = stage(f0, std::min(chunk, T - f0));
+            const int nf = std::min(chunk, T - f0);
+            rc = stage(f0, nf);
+            if (!rc) rc = mark();
             if (rc) return rc;
-            dim3 grid(lg.ntx * lg.nty, std::min(chunk, T - f0));
+            dim3 grid(lg.ntx * lg.nty, nf);
             locate_tiles_kernel<<<grid, 256, P.smem_loc, st>>>(lg, b, f0);
             ctx->stats.launches += 1;
+            if (chunked && (rc = post(f0, nf))) return rc;
         }
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], st));
-    CK(cudaFuncSetAttribute(fallback_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_fb));
-    fallback_walk_kernel<<<ctx->num_sms * 4, 128, P.smem_fb, st>>>(P.lp, b, P.fb_win);
-    CK(cudaGetLastError());
-    CK(cudaFuncSetAttribute(finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_fin));
-    finalize_kernel<<<T, 512, P.smem_fin, st>>>(P.lp, b, P.sep, P.link);
-    CK(cudaGetLastError());
-    scan_frames_kernel<<<1, 1024, 0, st>>>(w.npart, w.off, T);
-    CK(cudaGetLastError());
-    ctx->stats.launches += 3;
+    if (!chunked) {
+        // the whole movie as one window: finalize, then link
+        fallback_walk_kernel<<<ctx->num_sms * 4, 128, P.smem_fb, st>>>(P.lp, b, P.fb_win, w.pbeg);
+        finalize_kernel<<<T, 512, P.smem_fin, st>>>(P.lp, b, P.sep, P.link, 0);
+        scan_frames_from_kernel<<<1, 1024, 0, st>>>(w.npart, w.off, 0, T);
+        CK(cudaGetLastError());
+        ctx->stats.launches += 3;
+    }
     CK(cudaEventRecord(ctx->ev[2], st));
     if (P.link) {
-        rc = run_link(ctx, P, w, st);
+        if (!chunked) rc = link_window(ctx, P, w, st, 0, T, 0);
+        if (!rc) rc = link_finish(ctx, P, w, st);
         if (rc) return rc;
     }
     CK(cudaEventRecord(ctx->ev[3], st));
@@ -714,9 +783,13 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
         unsigned long long ph[4];
         CK(cudaMemcpy(ph, w.phase_ns, sizeof(ph), cudaMemcpyDeviceToHost));
         for (int i = 0; i < 4; ++i) ctx->stats.link_phase_ms[i] = (float)(ph[i] * 1e-6);
-        int nd[9] = {0};
-        CK(cudaMemcpy(nd, w.ndirty, sizeof(int) * std::min(9, T + 2), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < 8; ++i) ctx->stats.link_dirty[i] = i + 1 < T + 2 ? nd[i + 1] : 0;
+        std::vector<int> nd((size_t)(T + 2) * std::max(wi, 1));
+        CK(cudaMemcpy(nd.data(), w.ndirty, sizeof(int) * nd.size(), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < 8; ++i) {
+            int v = 0;
+            for (int c = 0; c < std::max(wi, 1); ++c) v += i + 1 < T + 2 ? nd[(size_t)c * (T + 2) + i + 1] : 0;
+            ctx->stats.link_dirty[i] = v;
+        }
     }
     ctx->stats.fallback_walks = np;
     ctx->stats.particles = hb[4];
@@ -1000,8 +1073,8 @@ int enqueue_front(gt_ctx* ctx, BatchMovie& bm, const void* frames, cudaStream_t 
         }
     }
     CK(cudaGetLastError());
-    fallback_walk_kernel<<<ctx->num_sms, 128, P.smem_fb, s>>>(P.lp, b, P.fb_win);
-    finalize_kernel<<<T, 512, P.smem_fin, s>>>(P.lp, b, P.sep, P.link);
+    fallback_walk_kernel<<<ctx->num_sms, 128, P.smem_fb, s>>>(P.lp, b, P.fb_win, nullptr);
+    finalize_kernel<<<T, 512, P.smem_fin, s>>>(P.lp, b, P.sep, P.link, 0);
     scan_frames_kernel<<<1, 1024, 0, s>>>(w.npart, w.off, T);
     CK(cudaGetLastError());
     *launches += 3;
@@ -1072,6 +1145,7 @@ int enqueue_batch(gt_ctx* ctx, std::vector<BatchMovie>& B, gt_movie* mv, int n, 
         if (!B[i].solo) continue;
         BatchMovie& bm = B[i];
         CK(cudaMemsetAsync(bm.w.ndirty, 0, sizeof(int) * (bm.P.T + 2), st));
+        CK(cudaMemsetAsync(bm.w.phase_ns, 0, sizeof(unsigned long long) * 4, st));
         LinkBufs L = bm.solo_L;
         int memory = (int)bm.P.r.memory, max_passes = bm.P.T + 1, rounds = 0;
         int* nd = bm.w.ndirty;

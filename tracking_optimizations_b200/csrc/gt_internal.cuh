@@ -110,6 +110,7 @@ struct MovieBufs {
 
 struct LinkBufs {
     int T, cap_p, cap_m, cap_e, cap_s;
+    int tb, te;           // frames linked by this launch; earlier frames are final
     float r;              // search range
     int G, ncx, ncy;
     const float* py;

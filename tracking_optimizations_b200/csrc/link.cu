@@ -152,7 +152,7 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
     const int ncell = L.ncx * L.ncy;
     const int pool = L.lsm_bytes / 4;
 
-    for (int t = t0; t < L.T; t += tstride) {
+    for (int t = L.tb + t0; t < L.te; t += tstride) {
         if (only_dirty && !__ldcg(L.dirty + t)) continue;
         const int nd = L.npart[t];
         int* pred = L.pred + L.off[t];
@@ -442,7 +442,7 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
     const int cap_p = L.cap_p;
     const int nn = L.cap_s + cap_p;
     const int pool = L.lsm_bytes / 4;
-    for (int t = t0; t < L.T; t += tstride) {
+    for (int t = L.tb + t0; t < L.te; t += tstride) {
         const int fbeg = max(0, t - 1 - memory), fend = t - 2;
         if (fend < fbeg) continue;
         // number of candidates, to place the scratch
@@ -585,16 +585,16 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
 // between hops and the result is exact whatever the interleaving; particles
 // of early frames finish first and shorten the later walks.
 __device__ void roots_reset(const LinkBufs& L) {
-    const int n = L.off[L.T];
+    const int g0 = L.off[L.tb], n = L.off[L.te];
     const int stride = gridDim.x * blockDim.x;
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) L.root[g] = -1;
+    for (int g = g0 + blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) L.root[g] = -1;
 }
 
 __device__ void roots_walk(const LinkBufs& L) {
-    const int n = L.off[L.T];
+    const int g0 = L.off[L.tb], n = L.off[L.te];
     const int stride = gridDim.x * blockDim.x;
     volatile int* root = L.root;
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) {
+    for (int g = g0 + blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) {
         int r = g;
         while (true) {
             const int known = root[r];
@@ -635,7 +635,7 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_kernel(LinkBufs L, int m
     unsigned long long t0 = stamp ? gtimer() : 0, acc[4] = {0, 0, 0, 0};
     link_frames_body(L, 0, blockIdx.x, gridDim.x);
     int k = 0;
-    if (memory > 0 && L.T > 2) {
+    if (memory > 0 && L.te > 2) {
         for (k = 1; k <= max_passes; ++k) {
             grid.sync();
             if (stamp) { const unsigned long long t = gtimer(); acc[k == 1 ? 0 : 3] += t - t0; t0 = t; }
@@ -655,8 +655,8 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_kernel(LinkBufs L, int m
     grid.sync();  // so that the last stamp covers every block's walk
     if (stamp) {
         acc[1] += gtimer() - t0;
-        *passes = k;
-        for (int i = 0; i < 4; ++i) phase_ns[i] = acc[i];
+        *passes = max(*passes, k);  // several launches (frame windows) add up
+        for (int i = 0; i < 4; ++i) phase_ns[i] += acc[i];
     }
     (void)rounds;
 }

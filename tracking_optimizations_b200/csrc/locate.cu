@@ -310,11 +310,13 @@ __device__ float processed_at(const LocParams& p, const void* frames, size_t fba
     return res < 0.f ? 0.f : res;
 }
 
-__global__ void __launch_bounds__(128) fallback_walk_kernel(const LocParams p, const MovieBufs b, int win) {
+__global__ void __launch_bounds__(128) fallback_walk_kernel(const LocParams p, const MovieBufs b, int win,
+                                                            const int* pbeg) {
     extern __shared__ __align__(16) float wsm[];
     const int npend = *b.npend;
     const int n = 2 * win + 1;
-    for (int k = blockIdx.x; k < npend; k += gridDim.x) {
+    // entries from *pbeg on: those of the frames located since (chunked calls)
+    for (int k = (pbeg ? *pbeg : 0) + blockIdx.x; k < npend; k += gridDim.x) {
         const int code = b.pend[k];
         const int t = code / b.cap_c;
         Cand* rec = b.cand + code;

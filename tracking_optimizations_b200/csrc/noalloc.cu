@@ -25,8 +25,8 @@
 
 namespace gt {
 __global__ void locate_tiles_kernel(const LocParams p, const MovieBufs b, int frame0);
-__global__ void fallback_walk_kernel(const LocParams p, const MovieBufs b, int win);
-__global__ void finalize_kernel(const LocParams p, MovieBufs b, float sep, int link_grid);
+__global__ void fallback_walk_kernel(const LocParams p, const MovieBufs b, int win, const int* pbeg);
+__global__ void finalize_kernel(const LocParams p, MovieBufs b, float sep, int link_grid, int frame0);
 __global__ void scan_frames_kernel(const int* in, int* out, int n);
 __global__ void assemble_kernel(AsmArgs a);
 bool fast_supported(int kr, int dd, int rc, int diameter);
@@ -344,10 +344,10 @@ extern "C" int gt_locate_frame_static(const void* d_frame, int dtype, int H, int
     const int fb_win = std::min(100, std::max(lp.rint_c + 1, lp.max_iter - 1 + lp.rint_c + 1));
     const size_t smem_fb = sizeof(float) * (size_t)(2 * fb_win + 1) * (2 * fb_win + 1);
     SCK(cudaFuncSetAttribute(fallback_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fb));
-    fallback_walk_kernel<<<ds.num_sms * 4, 128, smem_fb, st>>>(lp, b, fb_win);
+    fallback_walk_kernel<<<ds.num_sms * 4, 128, smem_fb, st>>>(lp, b, fb_win, nullptr);
     SCK(cudaGetLastError());
     SCK(cudaFuncSetAttribute(finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * ncell)));
-    finalize_kernel<<<1, 512, 4 * ncell, st>>>(lp, b, (float)sep, 0);
+    finalize_kernel<<<1, 512, 4 * ncell, st>>>(lp, b, (float)sep, 0, 0);
     scan_frames_kernel<<<1, 1024, 0, st>>>(b.npart, off, 1);
     AsmArgs a;
     std::memset(&a, 0, sizeof(a));
