@@ -169,6 +169,17 @@ def test_memory_linking_exact(gpu, memory, seed):
     print(f"memory={memory}: link fixed-point passes {st['link_iterations']}")
 
 
+def test_linking_across_upload_chunks_exact(gpu):
+    """Host frames are uploaded, finalized and linked in chunks of 16 frames
+    here (the linker in frame windows); memory 4 with frequent blinking
+    reaches across the chunk boundaries, and the last chunk has 2 frames."""
+    spec = synth.MovieSpec(50, 128, 160, 50, 1.3, 200, 1200, 1.6, read_noise=5.0, blink=0.3, seed=77)
+    mv = synth.make_movie(spec)
+    check(mv, diameter=7, minmass=200, search_range=5.0, memory=4)
+    st = _native.last_stats()
+    assert st["link_iterations"] >= 1
+
+
 def test_dense_linking_subnets_exact(gpu):
     # DENSE_LINK density (20000 spots per 2048^2) on 512^2: many 2-12 subnets
     spec = synth.scaled(synth.DENSE_LINK, frames=8, height=512, width=512, seed=31)
