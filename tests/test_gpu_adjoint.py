@@ -115,6 +115,29 @@ def test_pixel_gradient_vs_torch_fp64(torch, adj, scene):
     assert np.all(g_gpu[g_ref == 0] == 0)
 
 
+def test_pixel_gradient_interior_tiles_vs_torch_fp64(torch, adj):
+    """A frame wide and tall enough for transpose tiles away from every edge
+    (the register-blocked interior passes) besides the edge tiles."""
+    spec = synth.scaled(synth.PLAIN_1000, frames=2, height=160, width=256, spots=60, seed=19)
+    f32 = synth.make_movie(spec).astype(np.float32)
+    frames = torch.from_numpy(f32).cuda()
+    rows, walk, names = adj.locate_with_walk(frames, D, noise_size=S, smoothing_size=K, **PARAMS)
+    wn = walk.cpu().numpy()
+    wk = wn[_kept(f32, wn)]
+    assert len(wk) > 40
+    rng = np.random.default_rng(8)
+    up = rng.normal(size=(len(wk), 3))
+    up[:, 2] *= 1e-3
+    g_gpu, gs_gpu, gk_gpu = _gpu_backward(torch, adj, frames, torch.from_numpy(wk).cuda(), up)
+    g_ref, gs_ref, gk_ref = adjoint_ref.torch_reference(f32, wk, up, D, S, K)
+    scale = np.abs(g_ref).max()
+    big = np.abs(g_ref) >= 1e-2 * scale
+    assert np.abs(g_gpu - g_ref).max() <= REL * scale
+    assert np.all(np.abs(g_gpu - g_ref)[big] <= REL * np.abs(g_ref)[big] + 1e-6 * scale)
+    assert abs(gs_gpu - gs_ref) <= REL * abs(gs_ref)
+    assert abs(gk_gpu - gk_ref) <= REL * abs(gk_ref)
+
+
 def test_pixel_gradient_vs_central_differences(torch, adj, scene):
     f32, frames, rows, walk = scene
     wn = walk.cpu().numpy()

@@ -274,9 +274,10 @@ __global__ void __launch_bounds__(TR_NT) adjoint_transpose_kernel(AdjParams p, c
     const int kr = KRT > 0 ? KRT : p.krad;
     const int H = p.H, W = p.W;
     const int SH = TR_TH + 2 * kr, SW = TR_TW + 2 * kr;
+    constexpr int RS = TR_TW + 1;  // row stride of the row-pass planes (odd: conflict-free column reads)
     float* S = tsm;               // SH x SW
-    float* RG = S + SH * SW;      // SH x TR_TW, Gaussian row pass
-    float* RB = RG + SH * TR_TW;  // SH x TR_TW, box row pass
+    float* RG = S + SH * SW;      // SH x RS, Gaussian row pass
+    float* RB = RG + SH * RS;     // SH x RS, box row pass
     const int ntx = (W + TR_TW - 1) / TR_TW;
     const int u0 = (blockIdx.x / ntx) * TR_TH, v0 = (blockIdx.x % ntx) * TR_TW;
     const int t = blockIdx.y;
@@ -291,22 +292,37 @@ __global__ void __launch_bounds__(TR_NT) adjoint_transpose_kernel(AdjParams p, c
     const bool cols_inner = v0 >= kr && v0 + TR_TW <= W - kr;
     const bool rows_inner = u0 >= kr && u0 + TR_TH <= H - kr;
     if (KRT > 0 && cols_inner) {
-        constexpr int TP = 2 * KRT + 1;
+        // 8 outputs of one row per item (taps loaded once), rows fastest
+        // across the lanes
+        constexpr int TP = 2 * KRT + 1, RF = 8, NCH = TR_TW / RF;
         float a[TP];
 #pragma unroll
         for (int j = 0; j < TP; ++j) a[j] = p.a[j];
-        for (int q = threadIdx.x; q < SH * TR_TW; q += TR_NT) {
-            const int r = q / TR_TW, c = q % TR_TW;
-            const float* srow = S + r * SW + c;
-            float g = 0.f, bx = 0.f;
+        for (int it = threadIdx.x; it < SH * NCH; it += TR_NT) {
+            const int ch = it / SH, r = it - ch * SH;
+            const int c0 = ch * RF;
+            const float* srow = S + r * SW + c0;
+            float v[RF + TP - 1];
 #pragma unroll
-            for (int j = 0; j < TP; ++j) {
-                const float v = srow[j];
-                g = fmaf(a[j], v, g);
-                bx = bx + v;
+            for (int i = 0; i < RF + TP - 1; ++i) v[i] = srow[i];
+            float* rg = RG + r * RS + c0;
+            float* rb = RB + r * RS + c0;
+#pragma unroll
+            for (int m = 0; m < RF; ++m) {
+                float g = 0.f;
+#pragma unroll
+                for (int j = 0; j < TP; ++j) g = fmaf(a[j], v[m + j], g);
+                rg[m] = g;
             }
-            RG[q] = g;
-            RB[q] = bx;
+            // direct sums, not a running difference: a window of zeros
+            // must give exactly zero (no gradient outside the particles)
+#pragma unroll
+            for (int m = 0; m < RF; ++m) {
+                float bs = 0.f;
+#pragma unroll
+                for (int j = 0; j < TP; ++j) bs = bs + v[m + j];
+                rb[m] = bs;
+            }
         }
     } else {
         for (int q = threadIdx.x; q < SH * TR_TW; q += TR_NT) {
@@ -322,28 +338,37 @@ __global__ void __launch_bounds__(TR_NT) adjoint_transpose_kernel(AdjParams p, c
                     if (pv >= 0 && pv < W) bx = fmaf((float)box_count(pv, qv, W, kr), v, bx);
                 }
             }
-            RG[q] = g;
-            RB[q] = bx;
+            RG[r * RS + c] = g;
+            RB[r * RS + c] = bx;
         }
     }
     __syncthreads();
     float* dst = gI + (size_t)t * H * W;
     const float ikk = 1.f / p.kk;
     if (KRT > 0 && rows_inner && v0 + TR_TW <= W) {
-        constexpr int TP = 2 * KRT + 1;
+        // 8 outputs of one column per item, columns fastest across the lanes
+        constexpr int TP = 2 * KRT + 1, CF = 8;
         float a[TP];
 #pragma unroll
         for (int j = 0; j < TP; ++j) a[j] = p.a[j];
-        for (int q = threadIdx.x; q < TR_TH * TR_TW; q += TR_NT) {
-            const int r = q / TR_TW, c = q % TR_TW;
-            float g = 0.f, bx = 0.f;
+        for (int it = threadIdx.x; it < TR_TW * (TR_TH / CF); it += TR_NT) {
+            const int c = it % TR_TW, r0 = (it / TR_TW) * CF;
+            float g[CF + TP - 1], b[CF + TP - 1];
 #pragma unroll
-            for (int i = 0; i < TP; ++i) {
-                const int rr = (r + i) * TR_TW + c;
-                g = fmaf(a[i], RG[rr], g);
-                bx = bx + RB[rr];
+            for (int i = 0; i < CF + TP - 1; ++i) {
+                g[i] = RG[(r0 + i) * RS + c];
+                b[i] = RB[(r0 + i) * RS + c];
             }
-            dst[(size_t)(u0 + r) * W + (v0 + c)] = fmaf(-bx, ikk, g);
+#pragma unroll
+            for (int m = 0; m < CF; ++m) {
+                float bs = 0.f;
+#pragma unroll
+                for (int i = 0; i < TP; ++i) bs = bs + b[m + i];
+                float gs = 0.f;
+#pragma unroll
+                for (int i = 0; i < TP; ++i) gs = fmaf(a[i], g[m + i], gs);
+                dst[(size_t)(u0 + r0 + m) * W + (v0 + c)] = fmaf(-bs, ikk, gs);
+            }
         }
     } else {
         for (int q = threadIdx.x; q < TR_TH * TR_TW; q += TR_NT) {
@@ -352,7 +377,7 @@ __global__ void __launch_bounds__(TR_NT) adjoint_transpose_kernel(AdjParams p, c
             if (qu >= H || qv >= W) continue;
             float g = 0.f, bx = 0.f;
             for (int i = -kr; i <= kr; ++i) {
-                const int rr = (r + kr + i) * TR_TW + c;
+                const int rr = (r + kr + i) * RS + c;
                 g = fmaf(p.a[i + kr], RG[rr], g);
                 const int pu = qu + i;
                 if (pu >= 0 && pu < H) bx = fmaf((float)box_count(pu, qu, H, kr), RB[rr], bx);
@@ -366,7 +391,7 @@ size_t adjoint_particle_smem(int K) { return sizeof(float) * (size_t)(2 * K + (A
 
 size_t adjoint_transpose_smem(int kr) {
     const int SH = TR_TH + 2 * kr, SW = TR_TW + 2 * kr;
-    return sizeof(float) * (size_t)(SH * SW + 2 * SH * TR_TW);
+    return sizeof(float) * (size_t)(SH * SW + 2 * SH * (TR_TW + 1));
 }
 
 cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* frames, const int* walk, long long n,
