@@ -11,15 +11,17 @@
 // every loop has a constant trip count.  One CTA per (frame, TH0 x 64 output
 // tile), 256 or 512 threads:
 //   0. the uint16 tile plus halo is staged by one TMA load (zero fill
-//      outside the frame) into U[RH][RW];
-//   1. U -> Rp: f32, rows interleaved in pairs (float2 = rows 2p, 2p+1);
-//   2. row pass: a thread filters one row pair over 8 columns (FFMA2 chains
-//      in tap order), Gaussian and boxcar -> Gp, Bp (row pairs);
-//   3. column pass: a thread filters one column over 8 rows (4 row pairs),
+//      outside the frame) into U[RH][US] (US >= RW: rows padded so that
+//      16-byte loads of consecutive row pairs spread over the banks);
+//   1. (no separate conversion) the row pass reads row pairs of U with
+//      16-byte loads, turns each u16 into an exact float (2^23 + u, minus
+//      2^23) and filters 8 columns per thread (FFMA2 chains in tap order),
+//      Gaussian and boxcar -> Gp, Bp (row pairs);
+//   2. column pass: a thread filters one column over 8 rows (4 row pairs),
 //      divides by the Gaussian norm and k^2, clips at 0 -> P2 (row pairs);
-//   4. row max over the dilation window (register sliding max) -> RM2;
-//   5. column max of RM2 compared with the centre -> local-max flags;
-//   6. the flagged pixels are listed by ballots and walked one per lane by
+//   3. row max over the dilation window (register sliding max) -> RM2;
+//   4. column max of RM2 compared with the centre -> local-max flags;
+//   5. the flagged pixels are listed by ballots and walked one per lane by
 //      as few warps as they need; those warps compute the features and
 //      emit the records (ranks from per-row bit masks, one slot atomic per
 //      warp).
@@ -72,19 +74,24 @@ struct Geo {
     static constexpr int NPW = (PW + FM - 1) / FM;
     static constexpr int PWC = FM * NPW;
     static constexpr int NRQ = (PH + FM - 1) / FM;
-    static constexpr int RPS = (PWC + 2 * KR) | 1;
     static constexpr int GPS = PWC | 1;
     static constexpr int P2S = PWC | 1;
     static constexpr int RMS = FT | 1;
     static constexpr int RPA = 4 * NRQ + KR;  // Gp/Bp row pairs allocated
-    static constexpr int SZ_RP = align128(cmax(RP * RPS * 8, 4 * NRQ * P2S * 8));
+    static constexpr int NV = (FM + 2 * KR + 7) / 8;  // 16-byte loads per raw row of a row-pass item
+    // raw tile row stride: a row pair spans an odd number of 16-byte units
+    // (quarter-warp 16-byte loads of consecutive row pairs hit 2 banks at most)
+    static constexpr int US = ((RW / 8) % 2 == 0) ? RW + 8 : RW;
+    static constexpr int SZ_P2 = align128(4 * NRQ * P2S * 8);
+    static constexpr int SZ_U = align128(RH * US * 2 + 16 * NV);  // + the last item's overrun
     static constexpr int SZ_GP = align128(cmax(cmax(RPA * GPS * 8, (PP + 1) * RMS * 8), TH0 * FT * 4));
-    static constexpr int SZ_BP = align128(cmax(cmax(RPA * GPS * 8, RH * RW * 2), TH0 * FT));
+    static constexpr int SZ_BP = align128(cmax(RPA * GPS * 8, TH0 * FT));
     static constexpr int K = circle_size(RC);
     static constexpr int SZ_TAB = align128(K * 8);
-    static constexpr int OFF_GP = SZ_RP;
-    static constexpr int OFF_BP = SZ_RP + SZ_GP;
-    static constexpr int OFF_TAB = SZ_RP + SZ_GP + SZ_BP;
+    static constexpr int OFF_GP = SZ_P2;
+    static constexpr int OFF_BP = OFF_GP + SZ_GP;
+    static constexpr int OFF_U = OFF_BP + SZ_BP;
+    static constexpr int OFF_TAB = OFF_U + SZ_U;
     static constexpr int SMEM = OFF_TAB + SZ_TAB;
     // index invariants of the phases below
     static_assert(((HP - O) & 1) == 0, "row pairs of the local-max pass must align");
@@ -95,8 +102,9 @@ struct Geo {
     static_assert(FT + HX <= PW, "centre columns computed");
     static_assert(4 * (NRQ - 1) + FM / 2 + KR <= RPA, "column pass reads allocated row pairs");
     static_assert((PH - 2) / 2 + KR <= RP - 1, "valid outputs read computed row pairs only");
-    static_assert(PWC + 2 * KR <= RPS && PWC <= GPS && PWC <= P2S && FT <= RMS, "row strides");
-    static_assert(RW <= 256 && RH <= 256, "TMA box");
+    static_assert(PWC <= GPS && PWC <= P2S && FT <= RMS, "row strides");
+    static_assert(US <= 256 && RH <= 256 && (US * 2) % 16 == 0, "TMA box");
+    static_assert((NPW - 1) * FM < US && (FM * 2) % 16 == 0, "16-byte raw loads start inside a U row");
     static_assert(SMEM <= 227 * 1024, "shared memory");
     static_assert(RC + 2 <= HP && RC <= HX, "walk and feature circles inside the processed region");
 };
@@ -298,11 +306,10 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     const int py0 = ty0 - HP, px0 = tx0 - HX;
     const int TH = min(TH0, H - ty0);
 
-    float2* Rp = (float2*)smem;
-    float2* P2 = Rp;  // P2 replaces Rp once the row pass is done
+    float2* P2 = (float2*)smem;
     float2* Gp = (float2*)(smem + G::OFF_GP);
     float2* Bp = (float2*)(smem + G::OFF_BP);
-    unsigned short* U = (unsigned short*)Bp;    // raw tile until converted
+    unsigned short* U = (unsigned short*)(smem + G::OFF_U);  // raw tile, row stride US
     float2* RM2 = Gp;                           // after the column pass
     int* clist = (int*)Gp;                      // after the local-max pass
     unsigned char* flags = (unsigned char*)Bp;  // after the column pass
@@ -316,7 +323,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         }
         __syncthreads();
         if (tid == 0) {
-            mbar_expect_tx(&bar, (uint32_t)(G::RH * G::RW * 2));
+            mbar_expect_tx(&bar, (uint32_t)(G::RH * G::US * 2));
             tma_load_3d(U, &tmap, &bar, rx0, ry0, t);
             bool done = false;
             for (int it = 0; it < (1 << 22) && !done; ++it) done = mbar_try_wait(&bar, 0);
@@ -332,8 +339,8 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         if (s_fail) return;
     } else {
         const unsigned short* fr = (const unsigned short*)b.frames + (size_t)t * H * W;
-        for (int i = tid; i < G::RH * G::RW; i += NTK) {
-            const int r = i / G::RW, c = i - r * G::RW;
+        for (int i = tid; i < G::RH * G::US; i += NTK) {
+            const int r = i / G::US, c = i - r * G::US;
             const int gy = ry0 + r, gx = rx0 + c;
             unsigned short v = 0;
             if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(fr + (size_t)gy * W + gx);
@@ -347,25 +354,32 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         for (int k = tid; k < G::K; k += NTK)
             sc[k] = make_float2(__ldg(b.char_tab + 3 * k + 1), __ldg(b.char_tab + 3 * k + 2));
 
-    // ---- 1. u16 -> f32 row pairs ----
-    for (int i = tid; i < G::RP * G::RW; i += NTK) {
-        const int pr = i / G::RW, c = i - pr * G::RW;
-        Rp[pr * G::RPS + c] = make_float2((float)U[(2 * pr) * G::RW + c], (float)U[(2 * pr + 1) * G::RW + c]);
-    }
-    __syncthreads();
-
     float2 W2[TAPS];
 #pragma unroll
     for (int j = 0; j < TAPS; ++j) W2[j] = make_float2(p.w[j], p.w[j]);
 
-    // ---- 2. row pass (preprocess_rows.wgsl) on row pairs ----
+    // ---- 1. row pass (preprocess_rows.wgsl) on row pairs ----
     for (int it = tid; it < G::RP * G::NPW; it += NTK) {
         const int q = it / G::RP, pr = it - q * G::RP;
         const int pc0 = q * FM;
-        const float2* src = Rp + pr * G::RPS + pc0;
-        float2 v[FM + 2 * KR];
+        // raw rows 2 pr and 2 pr + 1 as exact floats: 0x4B000000 | u is 2^23 + u
+        const uint4* r0 = (const uint4*)(U + (2 * pr) * G::US + pc0);
+        const uint4* r1 = (const uint4*)(U + (2 * pr + 1) * G::US + pc0);
+        float2 v[8 * G::NV];
 #pragma unroll
-        for (int i = 0; i < FM + 2 * KR; ++i) v[i] = src[i];
+        for (int l = 0; l < G::NV; ++l) {
+            const uint4 a4 = r0[l], c4 = r1[l];
+            const unsigned int wa[4] = {a4.x, a4.y, a4.z, a4.w}, wc[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const float2 lo = make_float2(__uint_as_float(__byte_perm(wa[h], 0x4B00u, 0x5410)),
+                                              __uint_as_float(__byte_perm(wc[h], 0x4B00u, 0x5410)));
+                const float2 hi = make_float2(__uint_as_float(__byte_perm(wa[h], 0x4B00u, 0x5432)),
+                                              __uint_as_float(__byte_perm(wc[h], 0x4B00u, 0x5432)));
+                v[8 * l + 2 * h] = add2(lo, make_float2(-8388608.f, -8388608.f));
+                v[8 * l + 2 * h + 1] = add2(hi, make_float2(-8388608.f, -8388608.f));
+            }
+        }
         float2* gd = Gp + pr * G::GPS + pc0;
         float2* bd = Bp + pr * G::GPS + pc0;
 #pragma unroll
@@ -395,7 +409,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
 #pragma unroll
                 for (int j = 0; j < TAPS; ++j) {
                     const int cc = clampi(reflect_once(fc - KR + j, W) - rx0, 0, G::RW - 1);
-                    s = add2(s, Rp[pr * G::RPS + cc]);
+                    s = add2(s, make_float2((float)U[(2 * pr) * G::US + cc], (float)U[(2 * pr + 1) * G::US + cc]));
                 }
                 bd[m] = s;
             }
@@ -403,7 +417,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     }
     __syncthreads();
 
-    // ---- 3. column pass (preprocess_cols.wgsl) -> P2 ----
+    // ---- 2. column pass (preprocess_cols.wgsl) -> P2 ----
     const float NEG = -CUDART_INF_F;
     for (int it = tid; it < G::PWC * G::NRQ; it += NTK) {
         const int rq = it / G::PWC, c = it - rq * G::PWC;
@@ -472,7 +486,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     }
     __syncthreads();
 
-    // ---- 4. row max over the dilation window (max_rows.wgsl) ----
+    // ---- 3. row max over the dilation window (max_rows.wgsl) ----
     for (int it = tid; it < G::PP * (FT / FM); it += NTK) {
         const int q = it / G::PP, pr = it - q * G::PP;
         const int tc0 = q * FM;
@@ -492,7 +506,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     }
     __syncthreads();
 
-    // ---- 5. column max vs centre: non-strict local max (walk_cols.wgsl:19-36) ----
+    // ---- 4. column max vs centre: non-strict local max (walk_cols.wgsl:19-36) ----
     for (int it = tid; it < FT * (TH0 / FM); it += NTK) {
         const int tc = it % FT, rq = it / FT;
         const int tr0 = rq * FM;
@@ -523,7 +537,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     }
     __syncthreads();
 
-    // ---- 6. candidate list, walks packed 32 per warp, emission ----
+    // ---- 5. candidate list, walks packed 32 per warp, emission ----
     // Each warp appends the flagged pixels of its own tile rows to the CTA
     // list; the list is then walked one candidate per lane by as few warps
     // as it needs (the other warps leave), so the walks, which are the
@@ -752,7 +766,7 @@ cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaSt
         using G = Geo<KR, DD, TH, RC>;                                                                  \
         CUtensorMap map;                                                                                \
         std::memset(&map, 0, sizeof(map));                                                              \
-        const int tma = make_tensor_map(&map, b.frames, T, p.H, p.W, G::RW, G::RH) ? 1 : 0;            \
+        const int tma = make_tensor_map(&map, b.frames, T, p.H, p.W, G::US, G::RH) ? 1 : 0;            \
         *used_tma = tma;                                                                                \
         cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD, TH, RC>,                         \
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);      \
