@@ -83,6 +83,8 @@ struct gt_ctx {
     cudaStream_t side[8] = {};
     cudaEvent_t bev[20] = {};         // fork/join events
     int* h_status = nullptr;          // pinned: 8 ints per movie
+    int* h_stage = nullptr;           // pinned: one call's statistics, read back in one go
+    size_t h_stage_n = 0;
     uint16_t* h_frames = nullptr;     // pinned: decoded file frames
     size_t h_frames_n = 0;
     size_t h_status_n = 0;
@@ -618,7 +620,8 @@ int fast_division(gt_ctx* ctx, const Plan& P, FixedDiv* dn, FixedDiv* dk, bool* 
 int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames, cudaStream_t st,
                  int* err_bits, int64_t* nrows, int* d_walk = nullptr, int64_t walk_rows = 0,
                  const void* h_frames = nullptr, size_t elem = 0,
-                 const std::function<int(int, int)>* ready = nullptr) {
+                 const std::function<int(int, int)>* ready = nullptr, float* d_out = nullptr,
+                 int64_t out_rows = 0) {
     const int T = P.T;
     MovieBufs b = movie_bufs(P, w, d_frames);
     int rc = upload_tables(ctx, P, w, st);
@@ -756,38 +759,53 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
     a.cand = w.cand; a.root = w.root; a.newid = w.newid;
     a.sig_off = w.sig_off; a.n_sig = (int)P.sig_off.size() / 2;
     a.bg_off = w.bg_off; a.n_bg = (int)P.bg_off.size() / 2;
-    a.out = w.out;
-    a.out_rows = LLONG_MAX;
+    // a caller's device buffer takes the rows directly (those beyond its
+    // capacity are not written; the caller learns the count)
+    a.out = d_out ? d_out : w.out;
+    a.out_rows = d_out ? out_rows : LLONG_MAX;
     a.walk = d_walk;
     a.walk_rows = walk_rows;
     assemble_kernel<<<T, 256, 0, st>>>(a);
     CK(cudaGetLastError());
     ctx->stats.launches += 1;
     CK(cudaEventRecord(ctx->ev[4], st));
-    int hb[5];
-    CK(cudaMemcpyAsync(hb, w.err, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(hb + 4, w.off + T, sizeof(int), cudaMemcpyDeviceToHost, st));
-    int np = 0;
-    CK(cudaMemcpyAsync(&np, w.npend, sizeof(int), cudaMemcpyDeviceToHost, st));
-    int nc_total = 0;
-    CK(cudaStreamSynchronize(st));
-    {
-        std::vector<int> fc(T);
-        CK(cudaMemcpy(fc.data(), w.fcount, sizeof(int) * T, cudaMemcpyDeviceToHost));
-        for (int v : fc) nc_total += v;
+    // every statistic of the call in one readback: error words, row count,
+    // pending walks, per-frame record counts, linker phases and dirty counts
+    const int nwin = std::max(wi, 1);
+    const size_t n_nd = P.link ? (size_t)(T + 2) * nwin : 0;
+    const size_t ph_off = (6 + (size_t)T + 1) & ~(size_t)1;  // 8-byte aligned for the phase times
+    const size_t need_ints = ph_off + 8 + n_nd;
+    if (ctx->h_stage_n < need_ints) {
+        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+        ctx->h_stage = nullptr;
+        ctx->h_stage_n = 0;
+        CK(cudaHostAlloc((void**)&ctx->h_stage, sizeof(int) * need_ints, cudaHostAllocDefault));
+        ctx->h_stage_n = need_ints;
     }
+    int* hs = ctx->h_stage;
+    CK(cudaMemcpyAsync(hs, w.err, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hs + 4, w.off + T, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hs + 5, w.npend, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hs + 6, w.fcount, sizeof(int) * T, cudaMemcpyDeviceToHost, st));
+    unsigned long long* hph = (unsigned long long*)(hs + ph_off);  // 4 u64
+    if (P.link) {
+        CK(cudaMemcpyAsync(hph, w.phase_ns, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hs + ph_off + 8, w.ndirty, sizeof(int) * n_nd, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    int hb[5] = {hs[0], hs[1], hs[2], hs[3], hs[4]};
+    const int np = hs[5];
+    long long nc_total = 0;
+    for (int t = 0; t < T; ++t) nc_total += hs[6 + t];
     *err_bits = hb[0];
     *nrows = hb[4];
     ctx->stats.link_iterations = P.link ? hb[1] : 0;
     if (P.link) {
-        unsigned long long ph[4];
-        CK(cudaMemcpy(ph, w.phase_ns, sizeof(ph), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < 4; ++i) ctx->stats.link_phase_ms[i] = (float)(ph[i] * 1e-6);
-        std::vector<int> nd((size_t)(T + 2) * std::max(wi, 1));
-        CK(cudaMemcpy(nd.data(), w.ndirty, sizeof(int) * nd.size(), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < 4; ++i) ctx->stats.link_phase_ms[i] = (float)(hph[i] * 1e-6);
+        const int* nd = hs + ph_off + 8;
         for (int i = 0; i < 8; ++i) {
             int v = 0;
-            for (int c = 0; c < std::max(wi, 1); ++c) v += i + 1 < T + 2 ? nd[(size_t)c * (T + 2) + i + 1] : 0;
+            for (int c = 0; c < nwin; ++c) v += i + 1 < T + 2 ? nd[(size_t)c * (T + 2) + i + 1] : 0;
             ctx->stats.link_dirty[i] = v;
         }
     }
@@ -910,15 +928,16 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
         if (rc) return rc;
         const size_t fbytes = host ? (size_t)T * H * W * elem_size(dtype) : 0;
         Work w{};
-        const size_t need = carve(P, nullptr, &w, fbytes, true);
+        // a caller's device buffer receives the rows directly: no table slab
+        const size_t need = carve(P, nullptr, &w, fbytes, true, d_out == nullptr);
         rc = ensure_arena(ctx, need);
         if (rc) return rc;
-        carve(P, ctx->arena, &w, fbytes, true);
+        carve(P, ctx->arena, &w, fbytes, true, d_out == nullptr);
         const void* dfr = host ? w.frames : frames;
         int bits = 0;
         int64_t nrows = 0;
         rc = run_pipeline(ctx, P, w, dfr, st, &bits, &nrows, d_walk, d_walk ? out_rows : 0, host ? frames : nullptr,
-                          elem_size(dtype), ready);
+                          elem_size(dtype), ready, d_out, out_rows);
         if (rc) return rc;
         bool retry;
         rc = err_status(ctx, bits, &retry);
@@ -943,12 +962,8 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
                 CK(cudaStreamSynchronize(st));
             }
         }
-        if (d_out) {
-            const int64_t n = std::min(nrows, out_rows);
-            if (n > 0)
-                CK(cudaMemcpyAsync(d_out, w.out, sizeof(float) * (size_t)n * ncols, cudaMemcpyDeviceToDevice, st));
-            CK(cudaStreamSynchronize(st));
-        }
+        // with d_out the rows were written there directly (run_pipeline
+        // returns after the stream is synchronised)
         if (nrows_out) *nrows_out = nrows;
         return GT_OK;
     }
@@ -1207,7 +1222,6 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
     // pinned status words, side streams, events
     if (ctx->h_status_n < (size_t)8 * n) {
         if (ctx->h_status) cudaFreeHost(ctx->h_status);
-    if (ctx->h_frames) cudaFreeHost(ctx->h_frames);
         ctx->h_status = nullptr;
         ctx->h_status_n = 0;
         CK(cudaHostAlloc((void**)&ctx->h_status, sizeof(int) * 8 * (size_t)n, cudaHostAllocDefault));
@@ -1661,6 +1675,7 @@ void gt_ctx_destroy(gt_ctx* ctx) {
         if (e) cudaEventDestroy(e);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     if (ctx->h_frames) cudaFreeHost(ctx->h_frames);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     for (auto& sd : ctx->side)
         if (sd) cudaStreamDestroy(sd);
     for (auto& e : ctx->bev)
