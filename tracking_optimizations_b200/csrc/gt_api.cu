@@ -84,6 +84,7 @@ struct gt_ctx {
     cudaEvent_t bev[20] = {};         // fork/join events
     int* h_status = nullptr;          // pinned: 8 ints per movie
     int* h_stage = nullptr;           // pinned: one call's statistics, read back in one go
+    int link_per_sm = 0;              // resident link_fixpoint_kernel blocks per SM (queried once)
     size_t h_stage_n = 0;
     uint16_t* h_frames = nullptr;     // pinned: decoded file frames
     size_t h_frames_n = 0;
@@ -521,10 +522,13 @@ int link_window(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st, int 
     const int T = P.T;
     int rounds = 0;
     L.lsm_bytes = LINK_POOL_BYTES;
-    CK(cudaFuncSetAttribute(link_fixpoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.lsm_bytes));
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_kernel, 256, L.lsm_bytes));
-    const int grid = std::max(1, std::min(P.nslot, per_sm * ctx->num_sms));
+    if (!ctx->link_per_sm) {
+        CK(cudaFuncSetAttribute(link_fixpoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.lsm_bytes));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_kernel, 256, L.lsm_bytes));
+        ctx->link_per_sm = std::max(1, per_sm);
+    }
+    const int grid = std::max(1, std::min(P.nslot, ctx->link_per_sm * ctx->num_sms));
     int memory = (int)P.r.memory;
     int max_passes = te - tb + 1;
     int* ndirty = w.ndirty + (size_t)wi * (T + 2);
