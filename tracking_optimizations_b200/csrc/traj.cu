@@ -149,14 +149,32 @@ __global__ void msd_scatter_kernel(const unsigned long long* keys, int64_t n, co
     }
 }
 
-// one block per group, threads over lags
+// one block per (group, chunk of MSD_LAGS lags), threads over the lags:
+// the lags of a long-lived particle spread over several blocks
+constexpr int MSD_LAGS = 128;
+__global__ void msd_chunks_kernel(const int64_t* glags, int64_t ngroups, int64_t* gchunks) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += (int64_t)gridDim.x * blockDim.x)
+        gchunks[g] = (glags[g] + MSD_LAGS - 1) / MSD_LAGS;
+}
+
 __global__ void msd_kernel(const float2* pos, const int* taken, const int64_t* gbase, const int64_t* gspan,
-                           const int64_t* glags, const int64_t* gout, int64_t ngroups, float* msd) {
-    for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+                           const int64_t* glags, const int64_t* gout, const int64_t* cstart, int64_t ngroups,
+                           int64_t nchunks, float* msd) {
+    for (int64_t it = blockIdx.x; it < nchunks; it += gridDim.x) {
+        // the group whose chunk range [cstart[g], cstart[g + 1]) holds it
+        int64_t lo = 0, hi = ngroups - 1;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) / 2;
+            if (cstart[mid] <= it) lo = mid;
+            else hi = mid - 1;
+        }
+        const int64_t g = lo;
         const float2* p = pos + gbase[g];
         const int* tk = taken + gbase[g];
         const int64_t span = gspan[g], nl = glags[g];
-        for (int64_t L = 1 + threadIdx.x; L <= nl; L += blockDim.x) {
+        const int64_t L0 = 1 + (it - cstart[g]) * MSD_LAGS;
+        const int64_t L1 = min(nl, L0 + MSD_LAGS - 1);
+        for (int64_t L = L0 + threadIdx.x; L <= L1; L += blockDim.x) {
             double sx = 0.0, sy = 0.0;
             int64_t cnt = 0;
             for (int64_t i = 0; i + L < span; ++i) {
@@ -445,11 +463,19 @@ int traj_imsd(const int64_t* h_ids, const int64_t* h_frames, const float* h_x, c
         int64_t* eidx2 = B.get<int64_t>(tot_out);
         unsigned long long* nv = B.get<unsigned long long>(1);
         TA(msd && ekeys && ekeys2 && eidx && eidx2 && nv);
+        int64_t* gch = B.get<int64_t>(2 * (size_t)G);
+        TA(gch);
+        msd_chunks_kernel<<<grid, 256, 0, st>>>(glags, G, gch);
+        TK(cudaGetLastError());
+        int64_t nchunks = 0;
+        rc = exclusive_sum(gch, gch + G, G, B, st, &nchunks, msg);
+        if (rc) return rc;
+        const int gc = (int)std::min<int64_t>(std::max<int64_t>(nchunks, 1), (int64_t)num_sms * 64);
         cudaEvent_t e0, e1;
         TK(cudaEventCreate(&e0));
         TK(cudaEventCreate(&e1));
         TK(cudaEventRecord(e0, st));
-        msd_kernel<<<gg, 128, 0, st>>>(pos, taken, gbase, gspan, glags, gout, G, msd);
+        msd_kernel<<<gc, MSD_LAGS, 0, st>>>(pos, taken, gbase, gspan, glags, gout, gch + G, G, nchunks, msd);
         TK(cudaEventRecord(e1, st));
         TK(cudaGetLastError());
         msd_keys_kernel<<<gg, 128, 0, st>>>(msd, gout, glags, Gr.keys, Gr.gstart, G, ekeys, eidx);
