@@ -639,7 +639,8 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         for (int r = lane; r < TH; r += 32)
             b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = __popcll(rowmask[r]);
 
-    // emission: round 0 from the walks above, later rounds pending
+    // emission: the first stride of the list from the walks above, later
+    // strides as pending records
     const unsigned short* frame = (const unsigned short*)b.frames + (size_t)t * H * W;
     GRawAcc racc{frame, W};
     gbase = __shfl_sync(0xffffffffu, gbase, 0);
