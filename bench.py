@@ -9,6 +9,13 @@ search_range 5, memory 2, cpu_processed=True.  A step = locate + link of the
 whole movie.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload locate-link|adjoint|batched|file|postprocess]
+
+The other workloads print one line each: the adjoint of bandpass + refine
+at fixed peaks (256 x 512x512 f32), 64 uneven movies in one graph launch
+against per-movie calls, the movie from a multi-page TIFF file, and the
+lab pipeline's post-processing (stub filter, step lengths, per-particle
+MSD) of the movie's linked table.
 
 N > 1 runs under torchrun: every rank processes its own movie (weak scaling,
 no collective on the data path); the time is the max over ranks.
