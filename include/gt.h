@@ -263,30 +263,45 @@ GT_API int gt_steps(gt_ctx* ctx, const int64_t* ids, const float* x, const float
 GT_API int gt_imsd(gt_ctx* ctx, const int64_t* ids, const int64_t* frames, const float* x, const float* y,
                    int64_t n, double mpp, int64_t max_lagtime, gt_table* out);
 
-/* Locate (no linking) ONE device-resident frame while allocating nothing:
- * for callers that must not call cudaMalloc -- code running during CUDA
- * stream capture, processes whose device memory belongs to another
- * framework's pool, acquisition loops that forbid allocation once running.
+/* Locate (no linking) ONE device-resident frame while allocating nothing,
+ * for callers that cannot call cudaMalloc: processes whose device memory
+ * belongs to another framework's pool (an allocation beside it can fail or
+ * fragment it) and acquisition loops that forbid allocation once running.
  * No counterpart in the reference.  Frames up to 2^20 pixels (H, W <= 8192)
- * and 32768 features before the separation filter; sig_radius/bg_radius
- * <= 31; search_range must be unset.  Writes min(*nrows, out_rows) rows of
- * the gt_batch_device columns to d_out (device) and the row count to
- * *nrows, on `stream` (a cudaStream_t, NULL = default stream), returning
- * after the work has finished.  Scratch lives in one 16 MiB __device__ array
- * per GPU, held until the process exits and shared by every call, which
- * clears what must start at zero: calls that overlap on a GPU (other
- * streams, other host threads) race and must be serialised by the caller.
- * The first call on a device looks up that array's address; make it before
- * any stream capture.  Errors: gt_last_error(NULL). */
+ * and 32768 features before the separation filter (more is
+ * GT_ERR_CAPACITY); sig_radius/bg_radius <= 31; search_range must be unset.
+ * Writes min(*nrows, out_rows) rows of the gt_batch_device columns to d_out
+ * (device) and the row count to *nrows, on `stream` (a cudaStream_t, NULL =
+ * default stream), returning after the work has finished: the call waits on
+ * the stream and reads its row count back to the host, so it must not be
+ * made while that stream is being captured into a CUDA graph.  Scratch
+ * lives in one 16 MiB __device__ array per GPU, held until the process
+ * exits and shared by every call, which clears what must start at zero:
+ * calls that overlap on one GPU (other streams, other host threads) race on
+ * it and must be serialised by the caller.  The first call on a device looks
+ * up that array's address (under a lock, so threads may call concurrently
+ * for different GPUs).  Errors: gt_last_error(NULL) of the calling thread. */
 GT_API int gt_locate_frame_static(const void* d_frame, int dtype, int H, int W, const gt_params* params,
                                   float* d_out, int64_t out_rows, int64_t* nrows, void* stream);
 
 /* Free a table returned by gt_batch. */
 GT_API void gt_table_free(gt_table* table);
 
-/* Tuning options of a context (no reference counterpart):
+/* Options of a context (no reference counterpart):
  *   "locate_tile_rows"  output tile height of the specialised locate kernel, 32 or 64
  *   "force_generic"     1 = always use the generic locate kernel
+ *   "autotune"          0 = gt_batch_many_device keeps the configured tile rows
+ *   "normalized_taps"   1 = Gaussian taps divided by their sum on the host and
+ *                       no division in the passes (kernels.rs:86-97 gauss_1d,
+ *                       the form of the reference's own mass-plane dump);
+ *                       0 (default) = the live shaders' in-pass normalisation
+ *   "subnet_budget"     option trials per linking subnetwork before
+ *                       GT_ERR_SUBNET_BUDGET (0 = the default, 2^26)
+ *   "test_withhold_tile_copy"
+ *                       1 = the specialised locate kernel issues no TMA copy of
+ *                       its tiles, so its bounded wait runs out after a short
+ *                       limit and the call returns GT_ERR_DEVICE_TIMEOUT (a
+ *                       test of the timeout path; no fault, nothing in flight)
  * Returns GT_ERR_ARG for an unknown key or value. */
 GT_API int gt_ctx_set_option(gt_ctx* ctx, const char* key, int value);
 

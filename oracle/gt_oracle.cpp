@@ -17,6 +17,7 @@
 #include <cstring>
 #include <deque>
 #include <functional>
+#include <type_traits>
 #include <limits>
 #include <string>
 #include <thread>
@@ -44,14 +45,35 @@ template <typename F>
 struct Weights {
     std::vector<F> w;  // taps i = -rint..rint
     F norm = 0;
+    F rn = 1;          // reciprocal of norm, by which the passes multiply
     int rint = 0;
 };
 
+// The reference's GPU evaluates a WGSL division `a / b` as a multiplication
+// by the reciprocal of b, and contracts `a - b * c` into one fused
+// multiply-add.  Both are pinned by the reference's own dump of the mass
+// plane (gpu-tracking/masses.bin over gpu-tracking/inp, d = 9,
+// smoothing_size = 9, noise_size = 1), which this restatement reproduces on
+// all 419,200 pixels (tests/test_reference_dump.py): the boxcar term
+// `constant_sum / f32(k*k)` of preprocess_cols.wgsl:54 is
+// fma(-constant_sum, RN(1/k^2), gauss).  The reciprocal is taken as the
+// correctly rounded one (the dump pins it for k^2 = 81).  The FP64 twin
+// divides exactly: it is the accuracy reference.
+template <typename F>
+inline F gpu_div(F a, F b) {
+    if constexpr (std::is_same<F, float>::value) return a * (1.0f / b);
+    else return a / b;
+}
+
 // preprocess_rows.wgsl:30-45: gauss = exp(-x*x / (2*sigma2)), sigma2 is the
 // `noise_size` parameter itself (gpu_setup.rs:52), gauss_norm accumulates
-// every tap in order -rint..rint.
+// every tap in order -rint..rint.  With `normalized` the taps are instead
+// divided by their sum on the host and the passes do not divide
+// (kernels.rs:86-97 `gauss_1d`, the form of the shaders' commented-out
+// `gauss1d` binding, preprocess_rows.wgsl:7-8, preprocess_cols.wgsl:4-5,49):
+// the form in which the reference produced its dump of the mass plane.
 template <typename F>
-Weights<F> gauss_weights(int smoothing_size, float noise_size) {
+Weights<F> gauss_weights(int smoothing_size, float noise_size, int normalized) {
     Weights<F> W;
     W.rint = smoothing_size / 2;
     F sigma2 = (F)noise_size;
@@ -61,6 +83,12 @@ Weights<F> gauss_weights(int smoothing_size, float noise_size) {
         W.w.push_back(g);
         W.norm = W.norm + g;
     }
+    if (normalized) {
+        for (auto& g : W.w) g = g / W.norm;  // kernels.rs:19-22 normalize
+        W.rn = 1;
+    } else {
+        W.rn = std::is_same<F, float>::value ? (F)1 / W.norm : (F)1;
+    }
     return W;
 }
 
@@ -68,8 +96,9 @@ Weights<F> gauss_weights(int smoothing_size, float noise_size) {
 // Gaussian taps are zero-padded (skipped) but normalised by the full window
 // sum; the boxcar is reflect-padded and divided by f32(k*k).
 template <typename F>
-void bandpass(const float* pic, int H, int W, int k, float noise_size, F* out) {
-    Weights<F> G = gauss_weights<F>(k, noise_size);
+void bandpass(const float* pic, int H, int W, int k, float noise_size, int normalized, F* out) {
+    Weights<F> G = gauss_weights<F>(k, noise_size, normalized);
+    const bool f32 = std::is_same<F, float>::value;
     const int rint = G.rint;
     std::vector<F> tg((size_t)H * W), tb((size_t)H * W);
     for (int u = 0; u < H; ++u) {
@@ -84,11 +113,13 @@ void bandpass(const float* pic, int H, int W, int k, float noise_size, F* out) {
                 if (dg) gs = std::fma(G.w[i + rint], val, gs);
                 cs = cs + val;
             }
-            tg[(size_t)u * W + v] = gs / G.norm;
+            // preprocess_rows.wgsl:52 gauss_sum / gauss_norm
+            tg[(size_t)u * W + v] = f32 ? gs * G.rn : (normalized ? gs : gs / G.norm);
             tb[(size_t)u * W + v] = cs;
         }
     }
     const F kk = (F)(k * k);
+    const F rkk = (F)1 / kk;
     for (int u = 0; u < H; ++u) {
         for (int v = 0; v < W; ++v) {
             F gs = 0, cs = 0;
@@ -101,7 +132,8 @@ void bandpass(const float* pic, int H, int W, int k, float noise_size, F* out) {
                 if (dg) gs = std::fma(G.w[i + rint], tg[idx], gs);
                 cs = cs + tb[idx];
             }
-            F res = gs / G.norm - cs / kk;
+            // preprocess_cols.wgsl:54 gauss_sum/gauss_norm - constant_sum/f32(k*k)
+            F res = f32 ? std::fma(-cs, rkk, gs * G.rn) : (normalized ? gs : gs / G.norm) - cs / kk;
             out[(size_t)u * W + v] = res < (F)0 ? (F)0 : res;
         }
     }
@@ -175,13 +207,14 @@ struct Centers {
         if (want_char) {
             es = es * es;
             ec = ec * ec;
-            ecc[idx] = std::sqrt(es + ec) / (m - P[idx]);
-            rg[idx] = std::sqrt(Rg / m);
+            ecc[idx] = gpu_div<F>(std::sqrt(es + ec), m - P[idx]);
+            rg[idx] = std::sqrt(gpu_div<F>(Rg, m));
             rawm[idx] = rm;
             sig[idx] = s;
         }
-        c0[idx] = a0 / m;
-        c1[idx] = a1 / m;
+        // centers.wgsl:82-83 centers /= mass
+        c0[idx] = gpu_div<F>(a0, m);
+        c1[idx] = gpu_div<F>(a1, m);
         mass[idx] = m;
     }
 };
@@ -283,7 +316,7 @@ std::vector<Feature> locate_frame(const float* pic, int H, int W, const or_param
                                   const Circle& cc, const Circle& gc, bool filter = true) {
     const size_t n = (size_t)H * W;
     std::vector<F> P(n);
-    bandpass<F>(pic, H, W, p.smoothing_size, p.noise_size, P.data());
+    bandpass<F>(pic, H, W, p.smoothing_size, p.noise_size, p.normalized_taps, P.data());
 
     int D, o;
     derive_dilation(p.separation, &D, &o);
@@ -735,8 +768,24 @@ int or_link(const float* rows, int64_t n, int ncols, float search_range, int mem
 }
 
 void or_bandpass(const float* frame, int H, int W, int smoothing_size, float noise_size,
-                 float* processed) {
-    bandpass<float>(frame, H, W, smoothing_size, noise_size, processed);
+                 int normalized_taps, float* processed) {
+    bandpass<float>(frame, H, W, smoothing_size, noise_size, normalized_taps, processed);
+}
+
+void or_centers(const float* frame, int H, int W, const or_params* p, float* c0, float* c1, float* mass) {
+    // The centers/masses planes of centers.wgsl:88-109 at every pixel.
+    std::vector<float> P((size_t)H * W);
+    bandpass<float>(frame, H, W, p->smoothing_size, p->noise_size, p->normalized_taps, P.data());
+    Centers<float> C;
+    C.init(P.data(), frame, H, W, p->diameter, false, nullptr, nullptr);
+    for (int u = 0; u < H; ++u)
+        for (int v = 0; v < W; ++v) {
+            C.eval(u, v);
+            const size_t i = (size_t)u * W + v;
+            c0[i] = C.c0[i];
+            c1[i] = C.c1[i];
+            mass[i] = C.mass[i];
+        }
 }
 
 void or_locate_planes(const float* frame, int H, int W, const or_params* pp, float* planes) {

@@ -6,18 +6,27 @@
  * cpu_baseline leg (and its `--impl reference` arm) load it.  The product
  * library never links or calls it.
  *
- * Parity status: UNPINNED against the reference binary.  The reference's
- * GPU path is WGSL through wgpu (needs Vulkan/DX12/Metal; none exists here or
- * on the GPU hosts) and its host code is Rust (no cargo/rustc here), and the
- * reference ships no tests or golden vectors for this path.  The restatement
- * is pinned instead by hand-derived known-answer tests (tests/test_oracle_kat.py)
- * written from the reference source, and every function below cites the
- * reference lines it restates.
+ * Parity status: PINNED against the reference's own output for the
+ * bandpass and centroid-mass stages.  The reference ships a dump of the
+ * masses plane of its GPU path (gpu-tracking/masses.bin, centers.wgsl over
+ * the 524 x 800 image gpu-tracking/inp, diameter 9, smoothing_size 9,
+ * noise_size 1, taps normalised on the host as kernels.rs:86-97 does), and
+ * this restatement reproduces it bit for bit on all 419,200 pixels
+ * (tests/test_reference_dump.py).  That dump fixes the reference GPU's
+ * arithmetic conventions, which the restatement follows everywhere:
+ *   - `acc += a * b` is a fused multiply-add (the compiler contracts it);
+ *   - a division `a / b` is a multiplication by the reciprocal of b (taken
+ *     correctly rounded), and `a - b / c` contracts into
+ *     fma(-b, 1/c, a).
+ * The rest of the path (walk, separation filter, linking) is integer/index
+ * work or host Rust code with IEEE arithmetic, restated line by line; the
+ * reference binary itself cannot run here (Rust host, WGSL through wgpu).
  *
- * Two documented choices where the reference itself is not reproducible:
- *   - `acc += a * b` in the WGSL shaders is evaluated as a fused multiply-add
- *     (SPIR-V permits contraction; NVIDIA's Vulkan compiler contracts).
- *   - The third-party kd-tree 0.4.2 iteration order (separation-filter output
+ * Documented choices where the reference itself is not reproducible:
+ *   - the live shaders compute the Gaussian taps with the GPU's exp(); the
+ *     restatement takes the C library's expf (the dump, made with taps
+ *     from Rust's f32::exp on the host, does not pin the GPU's exp);
+ *   - the third-party kd-tree 0.4.2 iteration order (separation-filter output
  *     order, link neighbour order, new-ID order) is replaced by canonical
  *     raster order of each feature's originating pixel, and neighbour lists in
  *     ascending index order.
@@ -46,6 +55,8 @@ typedef struct or_params {
     int32_t has_bg_radius;
     float bg_radius;
     float gap_radius;
+    int32_t normalized_taps;  /* 1: taps divided by their sum on the host
+                                 (kernels.rs:86-97), no division in the passes */
 } or_params;
 
 /* Full locate (+ link when has_search_range) over T frames of f32 pixels.
@@ -71,7 +82,12 @@ int or_link(const float* rows, int64_t n, int ncols, float search_range,
 
 /* Bandpass of one frame (FP32 restatement); processed is H*W. */
 void or_bandpass(const float* frame, int H, int W, int smoothing_size,
-                 float noise_size, float* processed);
+                 float noise_size, int normalized_taps, float* processed);
+
+/* Dense centers (c0, c1) and masses planes of centers.wgsl at every pixel
+ * (H*W floats each; zeros in the border band). */
+void or_centers(const float* frame, int H, int W, const or_params* p, float* c0, float* c1,
+                float* mass);
 
 /* Raw results planes of the locate shaders for one frame: mass, y, x at the
  * originating pixel (3*H*W floats, zero where nothing was emitted). */

@@ -23,6 +23,7 @@ class OrParams(ctypes.Structure):
         ("has_search_range", ctypes.c_int32), ("search_range", ctypes.c_float), ("memory", ctypes.c_int32),
         ("has_sig_radius", ctypes.c_int32), ("sig_radius", ctypes.c_float),
         ("has_bg_radius", ctypes.c_int32), ("bg_radius", ctypes.c_float), ("gap_radius", ctypes.c_float),
+        ("normalized_taps", ctypes.c_int32),
     ]
 
 
@@ -52,7 +53,10 @@ def load():
         lib.or_link.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                 ctypes.c_void_p]
         lib.or_bandpass.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
-                                    ctypes.c_void_p]
+                                    ctypes.c_int, ctypes.c_void_p]
+        lib.or_centers.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrParams),
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.or_centers.restype = None
         lib.or_bandpass.restype = None
         lib.or_locate_planes.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrParams),
                                          ctypes.c_void_p]
@@ -71,8 +75,12 @@ NOT_IMPLEMENTED = ("maxsize", "threshold", "invert", "percentile", "topn", "prep
 def resolve(diameter, minmass=None, maxsize=None, separation=None, noise_size=None, smoothing_size=None,
             threshold=None, invert=None, percentile=None, topn=None, preprocess=None, max_iterations=None,
             characterize=None, filter_close=None, search_range=None, memory=None, cpu_processed=None,
-            sig_radius=None, bg_radius=None, gap_radius=None):
-    """lib.rs:73-91: reject unimplemented options, apply the defaults."""
+            sig_radius=None, bg_radius=None, gap_radius=None, normalized_taps=False):
+    """lib.rs:73-91: reject unimplemented options, apply the defaults.
+
+    normalized_taps selects the host-normalised Gaussian taps of
+    kernels.rs:86-97 (the form of the reference's mass-plane dump) instead of
+    the live shaders' in-pass normalisation."""
     loc = dict(maxsize=maxsize, threshold=threshold, invert=invert, percentile=percentile, topn=topn,
                preprocess=preprocess)
     for name in NOT_IMPLEMENTED:
@@ -95,6 +103,7 @@ def resolve(diameter, minmass=None, maxsize=None, separation=None, noise_size=No
     p.has_bg_radius = int(bg_radius is not None)
     p.bg_radius = 0.0 if bg_radius is None else float(bg_radius)
     p.gap_radius = 0.0 if gap_radius is None else float(gap_radius)
+    p.normalized_taps = int(bool(normalized_taps))
     return p
 
 
@@ -178,11 +187,22 @@ def link(table, search_range, memory=None):
     return ids
 
 
-def bandpass(frame, smoothing_size, noise_size):
+def bandpass(frame, smoothing_size, noise_size, normalized_taps=False):
     f = np.ascontiguousarray(frame, dtype=np.float32)
     out = np.empty_like(f)
     load().or_bandpass(f.ctypes.data_as(ctypes.c_void_p), f.shape[0], f.shape[1], int(smoothing_size),
-                       float(noise_size), out.ctypes.data_as(ctypes.c_void_p))
+                       float(noise_size), int(bool(normalized_taps)), out.ctypes.data_as(ctypes.c_void_p))
+    return out
+
+
+def centers(frame, diameter, **kw):
+    """Dense (c0, c1, mass) planes of centers.wgsl at every pixel."""
+    p = resolve(diameter, **kw)
+    f = np.ascontiguousarray(frame, dtype=np.float32)
+    out = np.zeros((3,) + f.shape, np.float32)
+    load().or_centers(f.ctypes.data_as(ctypes.c_void_p), f.shape[0], f.shape[1], ctypes.byref(p),
+                      out[0].ctypes.data_as(ctypes.c_void_p), out[1].ctypes.data_as(ctypes.c_void_p),
+                      out[2].ctypes.data_as(ctypes.c_void_p))
     return out
 
 

@@ -43,8 +43,9 @@ struct BpTerms {
 };
 
 // The bandpass at (u, v) in the operation order of the locate kernels
-// (row pass: fmaf over taps, divide by the tap sum; column pass likewise;
-// box sums in tap order), plus B and dG/ds in real-valued arithmetic.
+// (row pass: fmaf over taps, times the reciprocal of the tap sum; column
+// pass likewise, boxcar subtracted as fma(-box, 1/k^2, gauss); box sums in
+// tap order), plus B and dG/ds in real-valued arithmetic.
 __device__ __forceinline__ BpTerms bandpass_terms(const AdjParams& p, const float* fr, int u, int v) {
     const int kr = p.krad, H = p.H, W = p.W;
     float gs = 0.f, cs = 0.f, dg = 0.f;
@@ -68,7 +69,7 @@ __device__ __forceinline__ BpTerms bandpass_terms(const AdjParams& p, const floa
             }
             rb = rb + val;
         }
-        const float tg = rg / p.norm;
+        const float tg = rg * p.rn;
         if (in_r) {
             gs = fmaf(p.w[i + kr], tg, gs);
             dg = fmaf(p.da[i + kr], ra, dg);
@@ -77,8 +78,8 @@ __device__ __forceinline__ BpTerms bandpass_terms(const AdjParams& p, const floa
         cs = cs + rb;
     }
     BpTerms t;
-    t.r = gs / p.norm - cs / p.kk;
-    t.bmean = cs / p.kk;
+    t.r = fmaf(-cs, p.rkk, gs * p.rn);
+    t.bmean = cs * p.rkk;
     t.dg = dg;
     return t;
 }
@@ -166,8 +167,8 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
                 a1 = fmaf(data, (float)sci[2 * c + 1], a1);
                 mm = mm + data;
             }
-            c0 = a0 / mm;
-            c1 = a1 / mm;
+            c0 = __fmul_rn(a0, __frcp_rn(mm));  // centers.wgsl:82-83, a shader division
+            c1 = __fmul_rn(a1, __frcp_rn(mm));
             m = mm;
         }
         c0 = __shfl_sync(0xffffffffu, c0, 0);

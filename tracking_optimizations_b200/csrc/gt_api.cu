@@ -41,10 +41,8 @@ __global__ void grid_kernel(const float* py, const float* px, const int* npart, 
                             int ncy, int ncx, int* gstart, int* gidx);
 bool fast_supported(int kr, int dd, int rc, int diameter);
 cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaStream_t st, const LocParams& p,
-                               const MovieBufs& b, FixedDiv dnorm, FixedDiv dkk, int T, int frame0,
-                               int* used_tma);
-cudaError_t launch_verify_division(float divisor, FixedDiv f, unsigned int* d_count, int num_sms,
-                                   cudaStream_t st);
+                               const MovieBufs& b, int T, int frame0, int* used_tma);
+void gauss_taps(int smoothing_size, float noise_size, int normalized, float* w, float* norm, float* rn);
 cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* frames, const int* walk, long long n,
                                      const int* circ, const float* grad, float* yxm, float* gR, double* gpar,
                                      int* err, int num_sms, cudaStream_t st);
@@ -59,6 +57,30 @@ int traj_steps(const int64_t* h_ids, const float* h_x, const float* h_y, int64_t
 int traj_imsd(const int64_t* h_ids, const int64_t* h_frames, const float* h_x, const float* h_y, int64_t n,
               float mppf, int64_t max_lagtime, float* (*alloc)(size_t), float** out, int64_t* nout, float* ms_msd,
               cudaStream_t st, int num_sms, std::string* msg);
+
+// preprocess_rows.wgsl:44-45: taps exp(-i^2 / (2 * noise_size)) for
+// i = -k/2..k/2 and their running sum; the passes multiply by the
+// reciprocal of that sum (a shader division).  With `normalized` the taps
+// are divided by their sum on the host instead and the passes multiply by 1
+// (kernels.rs:86-97 `gauss_1d` and `normalize`, the form in which the
+// reference dumped its mass plane).
+void gauss_taps(int smoothing_size, float noise_size, int normalized, float* w, float* norm, float* rn) {
+    const int kr = smoothing_size / 2;
+    float s = 0.0f;
+    for (int i = -kr; i <= kr; ++i) {
+        const float x = (float)i;
+        const float g = std::exp(-x * x / (2.0f * noise_size));
+        w[i + kr] = g;
+        s = s + g;
+    }
+    *norm = s;
+    if (normalized) {
+        for (int i = 0; i < 2 * kr + 1; ++i) w[i] = w[i] / s;
+        *rn = 1.0f;
+    } else {
+        *rn = 1.0f / s;
+    }
+}
 }  // namespace gt
 
 using namespace gt;
@@ -72,8 +94,9 @@ struct gt_ctx {
     gt_stats stats{};
     int num_sms = 148;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    std::map<uint32_t, bool> div_ok;  // divisor bits -> fast division verified exact
-    unsigned int* d_count = nullptr;
+    int normalized_taps = 0;          // Gaussian taps divided by their sum on the host
+    long long subnet_budget = 1LL << 26;  // option trials per linking subnetwork
+    int withhold_tma = 0;             // test switch of the bounded tile-copy wait
     int force_generic = 0;            // always use locate_tiles_kernel
     int fast_tile_rows = 64;          // output tile height of the fast kernel (32 or 64)
     // batched path (gt_batch_many_device)
@@ -123,6 +146,7 @@ struct Resolved {
     uint32_t memory;
     int has_sig, has_bg;
     float sig_radius, bg_radius, gap_radius;
+    int normalized_taps;  // context option, not a reference parameter
 };
 
 int resolve(const gt_params* p, Resolved* r, std::string* msg) {
@@ -151,6 +175,7 @@ int resolve(const gt_params* p, Resolved* r, std::string* msg) {
     r->has_bg = p->has_bg_radius;
     r->bg_radius = p->bg_radius;
     r->gap_radius = p->has_gap_radius ? p->gap_radius : 0.0f;  // lib.rs:91
+    r->normalized_taps = 0;
     if (r->has_bg && !r->has_sig) {
         // execute_gpu.rs:301-333 only gathers raw pixels when sig_radius is
         // set; the reference then fails reshaping its output.
@@ -260,17 +285,9 @@ int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int 
     lp.krad = k / 2;
     lp.taps = 2 * lp.krad + 1;
     if (H <= lp.krad || W <= lp.krad) { *msg = "frame smaller than the smoothing window"; return GT_ERR_ARG; }
-    // preprocess_rows.wgsl:44-45 weights and their running sum
-    const float sigma2 = r.noise_size;
-    float norm = 0.0f;
-    for (int i = -lp.krad; i <= lp.krad; ++i) {
-        const float x = (float)i;
-        const float g = std::exp(-x * x / (2.0f * sigma2));
-        lp.w[i + lp.krad] = g;
-        norm = norm + g;
-    }
-    lp.norm = norm;
+    gauss_taps(k, r.noise_size, r.normalized_taps, lp.w, &lp.norm, &lp.rn);
     lp.kk = (float)(k * k);
+    lp.rkk = 1.0f / lp.kk;
     dilation(r.separation, &lp.D, &lp.o);
     lp.d = (int)r.diameter;
     lp.rint_c = ((int)r.diameter - 1) / 2;
@@ -287,11 +304,10 @@ int make_plan(const Resolved& r, int T, int H, int W, int dtype, int scale, int 
     lp.cpu_processed = r.cpu_processed;
     lp.characterize = r.characterize;
     lp.zero_skip = lp.max_iter >= 1 && lp.rint_c <= lp.o && lp.rint_c <= lp.D - 1 - lp.o;
+    lp.tma_spin = 1 << 22;
+    lp.tma_withhold = 0;
     P.fast = 0;
-    float wmin = 1.0f;
-    for (int i = 0; i < lp.taps; ++i) wmin = std::min(wmin, lp.w[i]);
-    const bool want_fast = dtype == GT_U16 && fast_supported(lp.krad, lp.D, lp.rint_c, lp.d) &&
-                           !force_generic_flag && wmin >= std::ldexp(1.0f, -40);
+    const bool want_fast = dtype == GT_U16 && fast_supported(lp.krad, lp.D, lp.rint_c, lp.d) && !force_generic_flag;
     P.char_tab.clear(); P.char_off.clear(); P.gchar_tab.clear();
     circle_tables(lp.char_r, P.char_tab, &P.char_off, 1);
     circle_tables(lp.rint_c, P.gchar_tab, nullptr, 0);
@@ -474,7 +490,7 @@ int ensure_arena(gt_ctx* ctx, size_t bytes) {
     return GT_OK;
 }
 
-LinkBufs link_bufs(const Plan& P, const Work& w) {
+LinkBufs link_bufs(const Plan& P, const Work& w, long long budget) {
     LinkBufs L{};
     L.tb = 0;
     L.te = P.T;
@@ -484,7 +500,7 @@ LinkBufs link_bufs(const Plan& P, const Work& w) {
     L.py = w.py; L.px = w.px; L.npart = w.npart; L.off = w.off; L.gstart = w.gstart; L.gidx = w.gidx;
     L.pred = w.pred; L.lnext = w.lnext; L.mlist = w.mlist; L.mcount = w.mcount; L.dirty = w.dirty;
     L.ndirty = w.ndirty; L.newrank = w.newrank; L.newcount = w.newcount; L.root = w.root; L.err = w.err;
-    L.budget = SUBNET_BUDGET;
+    L.budget = budget;
     L.nslot = P.nslot;
     L.s_y = w.s_y; L.s_x = w.s_x; L.s_h = w.s_h; L.s_deg = w.s_deg; L.e_dst = w.e_dst; L.e_w = w.e_w;
     L.d_cnt = w.d_cnt; L.d_src = w.d_src; L.d_w = w.d_w; L.uf = w.uf; L.c_nd = w.c_nd; L.c_ns = w.c_ns;
@@ -516,7 +532,7 @@ int link_prepare(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
 }
 
 int link_window(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st, int tb, int te, int wi) {
-    LinkBufs L = link_bufs(P, w);
+    LinkBufs L = link_bufs(P, w, ctx->subnet_budget);
     L.tb = tb;
     L.te = te;
     const int T = P.T;
@@ -586,36 +602,6 @@ MovieBufs movie_bufs(const Plan& P, const Work& w, const void* frames) {
     return b;
 }
 
-// Exhaustive check (cached per divisor) that the fixed-divisor division of
-// the fast kernel equals IEEE division on its dividend domain.
-int fast_division(gt_ctx* ctx, const Plan& P, FixedDiv* dn, FixedDiv* dk, bool* ok, cudaStream_t st) {
-    const float divs[2] = {P.lp.norm, P.lp.kk};
-    FixedDiv fdv[2];
-    bool all = true;
-    for (int i = 0; i < 2; ++i) {
-        const float b = divs[i];
-        fdv[i].y = 1.0f / b;
-        fdv[i].nb = -b;
-        uint32_t bits;
-        std::memcpy(&bits, &b, 4);
-        auto it = ctx->div_ok.find(bits);
-        if (it == ctx->div_ok.end()) {
-            if (!ctx->d_count) CK(cudaMalloc((void**)&ctx->d_count, sizeof(unsigned int)));
-            CK(cudaMemsetAsync(ctx->d_count, 0, sizeof(unsigned int), st));
-            CK(launch_verify_division(b, fdv[i], ctx->d_count, ctx->num_sms, st));
-            unsigned int bad = 0;
-            CK(cudaMemcpyAsync(&bad, ctx->d_count, sizeof(bad), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            it = ctx->div_ok.emplace(bits, bad == 0).first;
-        }
-        all = all && it->second;
-    }
-    *ok = all;
-    *dn = fdv[0];
-    *dk = fdv[1];
-    return GT_OK;
-}
-
 // The whole locate(+link) pipeline on device frames; table left in w.out.
 // With h_frames set, d_frames is the workspace copy of host frames: the
 // copy runs in chunks of frames on the context's copy stream and each
@@ -637,14 +623,7 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
     for (int i = 0; i < 5; ++i)
         if (!ctx->ev[i]) CK(cudaEventCreate(&ctx->ev[i]));
     const int ntiles = P.lp.ntx * P.lp.nty;
-    bool fast = P.fast != 0;
-    FixedDiv dn{}, dk{};
-    if (fast) {
-        bool ok = false;
-        rc = fast_division(ctx, P, &dn, &dk, &ok, st);
-        if (rc) return rc;
-        fast = ok;  // otherwise the generic kernel (IEEE division)
-    }
+    const bool fast = P.fast != 0;
     ctx->stats.locate_kernel = fast ? 1 : 0;
     // frame chunks: up to 16 for host frames (copy/locate overlap; the
     // locate of the last chunk is what remains after the copy), else as
@@ -713,8 +692,7 @@ int run_pipeline(gt_ctx* ctx, const Plan& P, const Work& w, const void* d_frames
             if (rc) return rc;
             dim3 grid(ntiles, nf);
             int used_tma = 0;
-            CK(launch_locate_fast(P.lp.krad, P.lp.D, P.lp.rint_c, P.fast_th, grid, st, P.lp, b, dn, dk, T, f0,
-                                  &used_tma));
+            CK(launch_locate_fast(P.lp.krad, P.lp.D, P.lp.rint_c, P.fast_th, grid, st, P.lp, b, T, f0, &used_tma));
             ctx->stats.launches += 1;
             ctx->stats.locate_kernel = used_tma ? 2 : 1;
             if (chunked && (rc = post(f0, nf))) return rc;
@@ -924,12 +902,17 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
     Resolved r;
     int rc = resolve(params, &r, &ctx->err);
     if (rc) return rc;
+    r.normalized_taps = ctx->normalized_taps;
     CK(cudaSetDevice(ctx->device));
     for (int scale = 1; scale <= 64; scale *= 4) {
         Plan P;
         rc = make_plan(r, T, H, W, dtype, scale, ctx->num_sms, &P, &ctx->err, ctx->force_generic,
                        ctx->fast_tile_rows);
         if (rc) return rc;
+        if (ctx->withhold_tma) {
+            P.lp.tma_withhold = 1;
+            P.lp.tma_spin = 1 << 10;
+        }
         const size_t fbytes = host ? (size_t)T * H * W * elem_size(dtype) : 0;
         Work w{};
         // a caller's device buffer receives the rows directly: no table slab
@@ -991,7 +974,6 @@ struct BatchMovie {
     Work w;
     size_t off = 0;
     bool fast = false;
-    FixedDiv dn{}, dk{};
     int link_slot = -1;  // index among the movies of the shared linker launch
     bool solo = false;   // linked by its own cooperative launch (large movie)
     LinkBufs solo_L{};
@@ -1038,8 +1020,8 @@ int tune_tile_rows(gt_ctx* ctx, BatchMovie& bm, const void* frames, cudaStream_t
                 CK(cudaMemsetAsync(bm.w.err, 0, sizeof(int) * 4, st));
                 CK(cudaEventRecord(ctx->ev[0], st));
                 int used_tma = 0;
-                CK(launch_locate_fast(Q.lp.krad, Q.lp.D, Q.lp.rint_c, ths[v], dim3(ntiles, nf), st, Q.lp, b, bm.dn,
-                                      bm.dk, P.T, 0, &used_tma));
+                CK(launch_locate_fast(Q.lp.krad, Q.lp.D, Q.lp.rint_c, ths[v], dim3(ntiles, nf), st, Q.lp, b, P.T, 0,
+                                      &used_tma));
                 CK(cudaEventRecord(ctx->ev[1], st));
                 CK(cudaEventSynchronize(ctx->ev[1]));
                 CK(cudaEventElapsedTime(&ms[v], ctx->ev[0], ctx->ev[1]));
@@ -1076,7 +1058,7 @@ int enqueue_front(gt_ctx* ctx, BatchMovie& bm, const void* frames, cudaStream_t 
         for (int f0 = 0; f0 < T; f0 += 65535) {
             int used_tma = 0;
             CK(launch_locate_fast(P.lp.krad, P.lp.D, P.lp.rint_c, P.fast_th, dim3(ntiles, std::min(65535, T - f0)), s,
-                                  P.lp, b, bm.dn, bm.dk, T, f0, &used_tma));
+                                  P.lp, b, T, f0, &used_tma));
             ++*launches;
         }
     } else {
@@ -1214,6 +1196,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         std::string msg;
         int rc = resolve(&m.params, &r, &msg);
         if (rc) { ctx->err = who + msg; return rc; }
+        r.normalized_taps = ctx->normalized_taps;
         rc = make_plan(r, m.T, m.H, m.W, m.dtype, 1, ctx->num_sms, &B[i].P, &msg, ctx->force_generic, ctx->fast_tile_rows,
                        ctx->batch_cap_div);
         if (rc) { ctx->err = who + msg; return rc; }
@@ -1237,17 +1220,8 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (int i = 0; i < 5; ++i)
         if (!ctx->ev[i]) CK(cudaEventCreate(&ctx->ev[i]));
-    // division checks and kernel choice (host-synchronous, before any capture)
-    for (int i = 0; i < n; ++i) {
-        BatchMovie& bm = B[i];
-        bm.fast = bm.P.fast != 0;
-        if (bm.fast) {
-            bool ok = false;
-            int rc = fast_division(ctx, bm.P, &bm.dn, &bm.dk, &ok, st);
-            if (rc) return rc;
-            bm.fast = ok;
-        }
-    }
+    // kernel choice
+    for (int i = 0; i < n; ++i) B[i].fast = B[i].P.fast != 0;
     // linked movies: a movie whose per-block scratch would cap the linker
     // grid below full residency is linked by its own launch (as in the
     // one-movie path); the others share one launch whose blocks share one
@@ -1396,7 +1370,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         int fs = 0;
         for (int i = 0; i < n; ++i) {
             if (B[i].link_slot < 0) continue;
-            LinkBufs L = link_bufs(B[i].P, B[i].w);
+            LinkBufs L = link_bufs(B[i].P, B[i].w, ctx->subnet_budget);
             L.nslot = (int)G;
             L.s_y = pool.s_y; L.s_x = pool.s_x; L.s_h = pool.s_h; L.s_deg = pool.s_deg;
             L.e_dst = pool.e_dst; L.e_w = pool.e_w; L.d_cnt = pool.d_cnt; L.d_src = pool.d_src; L.d_w = pool.d_w;
@@ -1420,7 +1394,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         Carver cb{big_base};
         slots(cb, pool_big, B[i].solo_grid, P.cap_s, (long long)P.cap_s + 1, (long long)P.cap_p + 1,
               (long long)P.cap_s + P.cap_p, P.cap_e, P.hsize);
-        LinkBufs L = link_bufs(B[i].P, B[i].w);
+        LinkBufs L = link_bufs(B[i].P, B[i].w, ctx->subnet_budget);
         L.nslot = B[i].solo_grid;
         L.s_y = pool_big.s_y; L.s_x = pool_big.s_x; L.s_h = pool_big.s_h; L.s_deg = pool_big.s_deg;
         L.e_dst = pool_big.e_dst; L.e_w = pool_big.e_w; L.d_cnt = pool_big.d_cnt; L.d_src = pool_big.d_src;
@@ -1564,19 +1538,15 @@ int adjoint_setup(gt_ctx* ctx, const float* d_frames, int T, int H, int W, const
     if (H <= ap->krad || W <= ap->krad) { ctx->err = "frame smaller than the smoothing window"; return GT_ERR_ARG; }
     const float sigma2 = r.noise_size;
     if (!(sigma2 > 0.0f)) { ctx->err = "noise_size must be > 0"; return GT_ERR_ARG; }
-    float norm = 0.0f;
+    gauss_taps(k, sigma2, ctx->normalized_taps, ap->w, &ap->norm, &ap->rn);
     double sw = 0.0, swi = 0.0;
     for (int i = -ap->krad; i <= ap->krad; ++i) {
-        const float x = (float)i;
-        const float g = std::exp(-x * x / (2.0f * sigma2));
-        ap->w[i + ap->krad] = g;
-        norm = norm + g;
         const double gd = std::exp(-(double)i * i / (2.0 * sigma2));
         sw += gd;
         swi += gd * i * i;
     }
-    ap->norm = norm;
     ap->kk = (float)(k * k);
+    ap->rkk = 1.0f / ap->kk;
     const double s2 = (double)sigma2 * sigma2;
     for (int i = -ap->krad; i <= ap->krad; ++i) {
         const double ai = std::exp(-(double)i * i / (2.0 * sigma2)) / sw;
@@ -1643,11 +1613,10 @@ int adjoint_finish(gt_ctx* ctx, const AdjWork& aw, cudaStream_t st) {
 
 namespace {
 thread_local std::string g_noctx_err;  // errors of calls made without a context
-const char* g_noctx_override = nullptr;  // message of gt_locate_frame_static
 }
 
 namespace gt {
-void set_noctx_override(const char* msg) { g_noctx_override = msg; }
+void set_noctx_error(const char* msg) { g_noctx_err = msg; }
 }  // namespace gt
 
 extern "C" {
@@ -1672,7 +1641,6 @@ void gt_ctx_destroy(gt_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->arena) cudaFree(ctx->arena);
-    if (ctx->d_count) cudaFree(ctx->d_count);
     if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     for (auto& e : ctx->cev)
@@ -1692,12 +1660,12 @@ void gt_ctx_destroy(gt_ctx* ctx) {
 
 const char* gt_last_error(const gt_ctx* ctx) {
     if (ctx) return ctx->err.c_str();
-    return g_noctx_override ? g_noctx_override : g_noctx_err.c_str();
+    return g_noctx_err.c_str();
 }
 
 int gt_column_names(const gt_params* params, char* buf, size_t buflen) {
     if (!params || !buf) return -GT_ERR_ARG;
-    g_noctx_override = nullptr;
+    g_noctx_err.clear();
     Resolved r;
     int rc = resolve(params, &r, &g_noctx_err);
     if (rc) return -rc;
@@ -1943,6 +1911,18 @@ int gt_ctx_set_option(gt_ctx* ctx, const char* key, int value) {
     if (k == "locate_tile_rows" && (value == 32 || value == 64)) { ctx->fast_tile_rows = value; return GT_OK; }
     if (k == "force_generic" && (value == 0 || value == 1)) { ctx->force_generic = value; return GT_OK; }
     if (k == "autotune" && (value == 0 || value == 1)) { ctx->tune_disabled = !value; return GT_OK; }
+    if (k == "subnet_budget" && value > 0) { ctx->subnet_budget = value; return GT_OK; }
+    if (k == "subnet_budget" && value == 0) { ctx->subnet_budget = SUBNET_BUDGET; return GT_OK; }
+    if (k == "test_withhold_tile_copy" && (value == 0 || value == 1)) { ctx->withhold_tma = value; return GT_OK; }
+    if (k == "normalized_taps" && (value == 0 || value == 1)) {
+        ctx->normalized_taps = value;
+        if (ctx->batch_exec) {  // the cached batch graph holds the old taps
+            cudaGraphExecDestroy(ctx->batch_exec);
+            ctx->batch_exec = nullptr;
+            ctx->batch_key.clear();
+        }
+        return GT_OK;
+    }
     ctx->err = "unknown option or value: " + k;
     return GT_ERR_ARG;
 }

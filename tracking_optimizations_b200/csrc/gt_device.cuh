@@ -4,7 +4,14 @@
 // every kernel variant produces identical bits.
 //
 // Compiled with --fmad=false: the only fused multiply-adds are the explicit
-// fmaf() calls, which stand for the shaders' `acc += a * b` statements.
+// fmaf() calls, which stand for the shaders' `acc += a * b` statements and
+// for `a - b / c`, which the reference's GPU contracts into fma(-b, 1/c, a).
+//
+// Division convention of the reference's GPU: a WGSL `a / b` is evaluated as
+// a multiplication by the reciprocal of b.  Both conventions are pinned by
+// the reference's own dump of its mass plane (gpu-tracking/masses.bin),
+// which the oracle reproduces bit for bit; the reciprocal is taken
+// correctly rounded.
 #pragma once
 #include <cuda_runtime.h>
 #include <math_constants.h>
@@ -20,6 +27,9 @@ __device__ __forceinline__ int reflect_once(int x, int n) {
 }
 
 __device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// A shader division a / b: a times the correctly rounded reciprocal of b.
+__device__ __forceinline__ float gpu_div(float a, float b) { return __fmul_rn(a, __frcp_rn(b)); }
 
 __device__ __forceinline__ float load_px(const void* frames, int dtype, size_t idx) {
     if (dtype == 0) return (float)__ldg((const unsigned short*)frames + idx);
@@ -57,8 +67,8 @@ __device__ __forceinline__ bool centroid_at(const LocParams& p, const Acc& P, in
             mm = mm + data;
         }
     }
-    c0 = a0 / mm;
-    c1 = a1 / mm;
+    c0 = gpu_div(a0, mm);  // centers.wgsl:82-83
+    c1 = gpu_div(a1, mm);
     m = mm;
     return true;
 }
@@ -164,8 +174,8 @@ __device__ __forceinline__ void gpu_features(const LocParams& p, const MovieBufs
     }
     es = es * es;
     ec = ec * ec;
-    c.g_ecc = sqrtf(es + ec) / (m - P(u, v));
-    c.g_rg = sqrtf(Rg / m);
+    c.g_ecc = gpu_div(sqrtf(es + ec), m - P(u, v));
+    c.g_rg = sqrtf(gpu_div(Rg, m));
     c.g_raw = rm;
     c.g_sig = s;
 }

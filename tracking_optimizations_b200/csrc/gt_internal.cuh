@@ -23,8 +23,11 @@ struct LocParams {
     int H, W;
     int taps, krad;             // smoothing window: taps = 2*krad + 1
     float w[GT_MAX_TAPS];       // exp(-i^2 / (2 * noise_size)), i = -krad..krad
-    float norm;                 // sum of w in order
+                                // (divided by norm when the taps are normalised on the host)
+    float norm;                 // sum of the exp() taps in order
     float kk;                   // f32(smoothing_size^2), the boxcar divisor
+    float rn;                   // RN(1 / norm), or 1 with host-normalised taps
+    float rkk;                  // RN(1 / kk)
     int D, o;                   // dilation size and window offset
     int d, rint_c, border;      // diameter, centroid radius (d-1)/2, border d/2
     int char_r;                 // cpu_processed circle radius d/2
@@ -37,6 +40,8 @@ struct LocParams {
     int zero_skip;              // zero-valued maxima provably have zero mass
     int n_char;                 // entries of the d/2 circle table
     int n_gchar;                // entries of the (d-1)/2 circle table
+    int tma_spin;               // iteration limit of the bounded wait for a staged tile
+    int tma_withhold;           // test switch: issue no tile copy, so the wait runs out
 };
 
 // One located feature, keyed by its originating pixel (walk_cols.wgsl:87-91).
@@ -67,14 +72,6 @@ enum ErrBits {
     ERR_SCRATCH_OVERFLOW = 32,
     ERR_DEVICE_TIMEOUT = 64,
 };
-
-// Division by a fixed divisor b: y = RN(1/b), nb = -b (see gt_simd.cuh).
-struct FixedDiv {
-    float y;
-    float nb;
-};
-
-
 
 // Per-movie device buffers and capacities.
 struct MovieBufs {
@@ -169,6 +166,7 @@ struct AdjParams {
     int K;                   // circle pixel count
     float w[GT_MAX_TAPS];    // forward weights, as LocParams::w
     float norm, kk;          // forward normaliser and f32(k * k)
+    float rn, rkk;           // their reciprocals, as LocParams
     float a[GT_MAX_TAPS];    // w_i / sum(w)
     float da[GT_MAX_TAPS];   // d a_i / d noise_size
     float k;                 // smoothing_size as a real number

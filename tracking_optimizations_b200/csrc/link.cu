@@ -110,7 +110,12 @@ __device__ bool solve_subnet(const LinkBufs& L, const int* dests, int nd, const 
             after_child = true;
             continue;
         }
-        if (++trials > L.budget) return false;
+        if (++trials > L.budget) {
+            // give back the sources the open levels hold
+            for (int q = 0; q < l; ++q)
+                if (cur[q] >= 0) used[cur[q]] = 0;
+            return false;
+        }
         const bool is_null = (o == nopt - 1);
         const float c = is_null ? null_cost : d_w[d_off[d] + o];
         score += c;

@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(NT) locate_tiles_kernel(const LocParams p, con
                     cs = cs + Rr[cc];
                 }
             }
-            Gr[r * PW + pc] = gs / p.norm;
+            Gr[r * PW + pc] = gs * p.rn;  // preprocess_rows.wgsl:52 gauss_sum / gauss_norm
             Br[r * PW + pc] = cs;
         }
     }
@@ -136,7 +136,8 @@ __global__ void __launch_bounds__(NT) locate_tiles_kernel(const LocParams p, con
                         cs = cs + Br[rr * PW + pc];
                     }
                 }
-                const float res = gs / p.norm - cs / p.kk;
+                // preprocess_cols.wgsl:54, contracted: fma(-cs, 1/k^2, gs / norm)
+                const float res = fmaf(-cs, p.rkk, gs * p.rn);
                 out = res < 0.f ? 0.f : res;
             }
             P[pr * PW + pc] = out;
@@ -302,11 +303,11 @@ __device__ float processed_at(const LocParams& p, const void* frames, size_t fba
             if (dgv) rg = fmaf(p.w[j + kr], val, rg);
             rb = rb + val;
         }
-        const float tg = rg / p.norm;
+        const float tg = rg * p.rn;
         if (dg) gs = fmaf(p.w[i + kr], tg, gs);
         cs = cs + rb;
     }
-    const float res = gs / p.norm - cs / p.kk;
+    const float res = fmaf(-cs, p.rkk, gs * p.rn);
     return res < 0.f ? 0.f : res;
 }
 

@@ -18,7 +18,8 @@
 //      2^23) and filters 8 columns per thread (FFMA2 chains in tap order),
 //      Gaussian and boxcar -> Gp, Bp (row pairs);
 //   2. column pass: a thread filters one column over 8 rows (4 row pairs),
-//      divides by the Gaussian norm and k^2, clips at 0 -> P2 (row pairs);
+//      scales by the reciprocal of the Gaussian norm, subtracts the boxcar
+//      as fma(-box, 1/k^2, gauss) and clips at 0 -> P2 (row pairs);
 //   3. row max over the dilation window (register sliding max) -> RM2;
 //   4. column max of RM2 compared with the centre -> local-max flags;
 //   5. the flagged pixels are listed by ballots and walked one per lane by
@@ -274,8 +275,8 @@ __device__ __forceinline__ bool centroid_fixed(const LocParams& p, const P2Acc<G
     float a0 = 0.f, a1 = 0.f, mm = 0.f;
     if (r0 & 1) circle_centroid<RC, 1, G::P2S>(P.P, base, a0, a1, mm);
     else circle_centroid<RC, 0, G::P2S>(P.P, base, a0, a1, mm);
-    c0 = a0 / mm;
-    c1 = a1 / mm;
+    c0 = gpu_div(a0, mm);  // centers.wgsl:82-83
+    c1 = gpu_div(a1, mm);
     m = mm;
     return true;
 }
@@ -284,8 +285,8 @@ __device__ __forceinline__ bool centroid_fixed(const LocParams& p, const P2Acc<G
 
 template <int KR, int DD, int TH0, int RC>
 __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
-    locate_fast_kernel(const LocParams p, const MovieBufs b, const FixedDiv dnorm, const FixedDiv dkk,
-                       const __grid_constant__ CUtensorMap tmap, int use_tma, int frame0) {
+    locate_fast_kernel(const LocParams p, const MovieBufs b, const __grid_constant__ CUtensorMap tmap, int use_tma,
+                       int frame0) {
     using G = Geo<KR, DD, TH0, RC>;
     constexpr int NTK = fast_threads(TH0);
     constexpr int TAPS = 2 * KR + 1;
@@ -324,15 +325,17 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         __syncthreads();
         if (tid == 0) {
             mbar_expect_tx(&bar, (uint32_t)(G::RH * G::US * 2));
-            tma_load_3d(U, &tmap, &bar, rx0, ry0, t);
+            // tma_withhold (a test of the timeout path) issues no copy: the
+            // barrier then never completes and the bounded wait runs out
+            if (!p.tma_withhold) tma_load_3d(U, &tmap, &bar, rx0, ry0, t);
             bool done = false;
-            for (int it = 0; it < (1 << 22) && !done; ++it) done = mbar_try_wait(&bar, 0);
+            for (int it = 0; it < p.tma_spin && !done; ++it) done = mbar_try_wait(&bar, 0);
             if (!done) {
                 atomicOr(b.err, ERR_DEVICE_TIMEOUT);
                 s_fail = 1;
                 // give the copy in flight a second bounded wait to land in
                 // this CTA's shared memory before the CTA exits
-                for (int it = 0; it < (1 << 22) && !done; ++it) done = mbar_try_wait(&bar, 0);
+                for (int it = 0; it < p.tma_spin && !done; ++it) done = mbar_try_wait(&bar, 0);
             }
         }
         __syncthreads();
@@ -357,6 +360,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     float2 W2[TAPS];
 #pragma unroll
     for (int j = 0; j < TAPS; ++j) W2[j] = make_float2(p.w[j], p.w[j]);
+    const float2 RN2 = make_float2(p.rn, p.rn), NRKK2 = make_float2(-p.rkk, -p.rkk);
 
     // ---- 1. row pass (preprocess_rows.wgsl) on row pairs ----
     for (int it = tid; it < G::RP * G::NPW; it += NTK) {
@@ -387,7 +391,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
             for (int j = 0; j < TAPS; ++j) acc = fma2(W2[j], v[m + j], acc);
-            gd[m] = div2(acc, dnorm);
+            gd[m] = mul2(acc, RN2);  // preprocess_rows.wgsl:52
         }
         const int fc0 = rx0 + pc0;  // frame column of v[0]
         if (fc0 >= 0 && fc0 + FM + 2 * KR - 1 < W) {
@@ -433,7 +437,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
             for (int j = 0; j < TAPS; ++j) acc = fma2(W2[j], (j & 1) ? ML[m + (j >> 1)] : L[m + (j >> 1)], acc);
-            gq[m] = div2(acc, dnorm);
+            gq[m] = mul2(acc, RN2);
         }
         float2 cs[FM / 2];
         const int fr0 = ry0 + 2 * p0;  // frame row of raw row 2*p0
@@ -472,7 +476,9 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         const bool all_in = cin && fa0 >= 0 && fa0 + FM - 1 < H;
 #pragma unroll
         for (int m = 0; m < FM / 2; ++m) {
-            const float2 res = sub2(gq[m], div2(cs[m], dkk));
+            // preprocess_cols.wgsl:54 contracted: fma(-cs, 1/k^2, gauss);
+            // cs * -rkk is exactly -(cs * rkk)
+            const float2 res = fma2(cs[m], NRKK2, gq[m]);
             float2 o;
             o.x = res.x < 0.f ? 0.f : res.x;  // preprocess_cols.wgsl:55-60
             o.y = res.y < 0.f ? 0.f : res.y;
@@ -698,25 +704,6 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     }
 }
 
-// Checks div1() against IEEE division for 0 and every binary32 dividend in
-// [2^-100, FLT_MAX].  Dividends of the fast kernel lie there: boxcar sums are
-// integers, and with every Gaussian weight >= 2^-40 (checked on the host) a
-// nonzero weighted sum of integer pixels is >= 2^-86.
-__global__ void verify_division_kernel(float divisor, FixedDiv f, unsigned int* mismatches) {
-    const unsigned int stride = gridDim.x * blockDim.x;
-    unsigned int bad = 0;
-    const unsigned int lo = 0x0d800000u;  // 2^-100
-    const unsigned int tid0 = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid0 == 0) bad += (__float_as_uint(div1(0.f, f)) != __float_as_uint(__fdiv_rn(0.f, divisor)));
-    for (unsigned int bits = lo + tid0; bits < 0x7f800000u; bits += stride) {
-        const float a = __uint_as_float(bits);
-        const float want = __fdiv_rn(a, divisor);
-        const float got = div1(a, f);
-        bad += (__float_as_uint(want) != __float_as_uint(got));
-    }
-    if (bad) atomicAdd(mismatches, bad);
-}
-
 namespace {
 // TMA descriptor over the movie (u16, dims W x H x T) with a box of the raw
 // tile.  Needs a 16-byte aligned base and a row pitch multiple of 16 bytes.
@@ -760,8 +747,7 @@ bool fast_supported(int kr, int dd, int rc, int diameter) {
 // Launches the specialised kernel over frames [frame0, frame0 + grid.y).
 // *used_tma reports whether the raw tiles were staged by TMA.
 cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaStream_t st, const LocParams& p,
-                               const MovieBufs& b, FixedDiv dnorm, FixedDiv dkk, int T, int frame0,
-                               int* used_tma) {
+                               const MovieBufs& b, int T, int frame0, int* used_tma) {
 #define GT_FAST_LAUNCH(KR, DD, RC, TH)                                                                  \
     {                                                                                                   \
         using G = Geo<KR, DD, TH, RC>;                                                                  \
@@ -772,7 +758,7 @@ cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaSt
         cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD, TH, RC>,                         \
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);      \
         if (e != cudaSuccess) return e;                                                                 \
-        locate_fast_kernel<KR, DD, TH, RC><<<grid, fast_threads(TH), G::SMEM, st>>>(p, b, dnorm, dkk, map, tma, frame0); \
+        locate_fast_kernel<KR, DD, TH, RC><<<grid, fast_threads(TH), G::SMEM, st>>>(p, b, map, tma, frame0); \
         return cudaGetLastError();                                                                      \
     }
 #define GT_FAST_CASE(KR, DD, RC)                                                                        \
@@ -784,12 +770,6 @@ cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaSt
 #undef GT_FAST_CASE
 #undef GT_FAST_LAUNCH
     return cudaErrorInvalidValue;
-}
-
-cudaError_t launch_verify_division(float divisor, FixedDiv f, unsigned int* d_count, int num_sms,
-                                   cudaStream_t st) {
-    verify_division_kernel<<<num_sms * 16, 256, 0, st>>>(divisor, f, d_count);
-    return cudaGetLastError();
 }
 
 }  // namespace gt

@@ -1,13 +1,16 @@
 // noalloc.cu -- gt_locate_frame_static: locate one device-resident frame
 // without allocating any memory.
 //
-// For callers that must not allocate: code running while a CUDA stream is
-// being captured into a graph (a cudaMalloc there breaks the capture), hosts
-// whose device memory is fully owned by another framework's pool, and
-// real-time acquisition loops that forbid allocation after start-up.  The
+// For callers that must not allocate device memory: hosts whose device
+// memory is fully owned by another framework's pool (a cudaMalloc beside it
+// can fail or fragment it), and real-time acquisition loops that forbid
+// allocation after start-up (an allocation can stall on the driver).  The
 // caller passes the frame and the output buffer; every other byte the call
 // needs lives in one file-scope __device__ array of kScratchBytes, which
-// each GPU that loads the library keeps until the process exits.
+// each GPU that loads the library keeps until the process exits.  The call
+// waits for its own work on the caller's stream and reads its row count
+// back to the host, so it must not be made while that stream is being
+// captured into a CUDA graph.
 //
 // The kernels are the ones gt_batch_device launches for the same frame
 // (locate, fallback walk, ordering and separation filter, output rows);
@@ -19,6 +22,7 @@
 #include <cstdio>
 #include <climits>
 #include <cstring>
+#include <mutex>
 
 #include "gt.h"
 #include "gt_internal.cuh"
@@ -31,11 +35,9 @@ __global__ void scan_frames_kernel(const int* in, int* out, int n);
 __global__ void assemble_kernel(AsmArgs a);
 bool fast_supported(int kr, int dd, int rc, int diameter);
 cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaStream_t st, const LocParams& p,
-                               const MovieBufs& b, FixedDiv dnorm, FixedDiv dkk, int T, int frame0,
-                               int* used_tma);
-cudaError_t launch_verify_division(float divisor, FixedDiv f, unsigned int* d_count, int num_sms,
-                                   cudaStream_t st);
-void set_noctx_override(const char* msg);
+                               const MovieBufs& b, int T, int frame0, int* used_tma);
+void gauss_taps(int smoothing_size, float noise_size, int normalized, float* w, float* norm, float* rn);
+void set_noctx_error(const char* msg);
 }  // namespace gt
 
 using namespace gt;
@@ -58,17 +60,14 @@ struct DeviceState {
     bool ready = false;
     unsigned char* scratch = nullptr;  // device address of g_scratch
     int num_sms = 0;
-    uint32_t div_bits[16];
-    bool div_ok[16];
-    int ndiv = 0;
 };
 
 DeviceState g_dev[kMaxDevices];
-char g_msg[256];  // last message of this entry point (calls are not thread-safe)
+std::mutex g_dev_mutex;  // guards the one-time set-up of each device
 
+// Messages go to the calling thread's context-free error (gt_last_error(NULL)).
 int fail(int status, const char* msg) {
-    std::snprintf(g_msg, sizeof(g_msg), "%s", msg);
-    set_noctx_override(g_msg);
+    set_noctx_error(msg);
     return status;
 }
 
@@ -76,8 +75,9 @@ int fail(int status, const char* msg) {
     do {                                                                          \
         cudaError_t e_ = (x);                                                     \
         if (e_ != cudaSuccess) {                                                  \
-            std::snprintf(g_msg, sizeof(g_msg), "%s: %s", #x, cudaGetErrorString(e_)); \
-            set_noctx_override(g_msg);                                            \
+            char m_[256];                                                         \
+            std::snprintf(m_, sizeof(m_), "%s: %s", #x, cudaGetErrorString(e_));  \
+            set_noctx_error(m_);                                                  \
             return GT_ERR_CUDA;                                                   \
         }                                                                         \
     } while (0)
@@ -142,8 +142,7 @@ struct Carve {
 
 extern "C" int gt_locate_frame_static(const void* d_frame, int dtype, int H, int W, const gt_params* pr,
                                       float* d_out, int64_t out_rows, int64_t* nrows, void* stream) {
-    g_msg[0] = 0;
-    set_noctx_override(g_msg);
+    set_noctx_error("");
     if (!d_frame || !pr || !nrows || (out_rows > 0 && !d_out)) return fail(GT_ERR_ARG, "null argument");
     if (dtype != GT_U16 && dtype != GT_F32) return fail(GT_ERR_ARG, "dtype must be GT_U16 or GT_F32");
     if (H < 1 || W < 1 || H > kMaxSide || W > kMaxSide || (long long)H * W > kMaxPixels)
@@ -172,14 +171,19 @@ extern "C" int gt_locate_frame_static(const void* d_frame, int dtype, int H, int
     int dev = 0;
     SCK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return fail(GT_ERR_ARG, "device index out of range");
-    DeviceState& ds = g_dev[dev];
-    if (!ds.ready) {
-        // once per device, with it current: the device address of the scratch
-        void* ptr = nullptr;
-        SCK(cudaGetSymbolAddress(&ptr, g_scratch));
-        SCK(cudaDeviceGetAttribute(&ds.num_sms, cudaDevAttrMultiProcessorCount, dev));
-        ds.scratch = (unsigned char*)ptr;
-        ds.ready = true;
+    DeviceState ds;
+    {
+        std::lock_guard<std::mutex> lock(g_dev_mutex);
+        DeviceState& gd = g_dev[dev];
+        if (!gd.ready) {
+            // once per device, with it current: the device address of the scratch
+            void* ptr = nullptr;
+            SCK(cudaGetSymbolAddress(&ptr, g_scratch));
+            SCK(cudaDeviceGetAttribute(&gd.num_sms, cudaDevAttrMultiProcessorCount, dev));
+            gd.scratch = (unsigned char*)ptr;
+            gd.ready = true;
+        }
+        ds = gd;
     }
     cudaStream_t st = (cudaStream_t)stream;
 
@@ -190,15 +194,9 @@ extern "C" int gt_locate_frame_static(const void* d_frame, int dtype, int H, int
     lp.krad = k / 2;
     lp.taps = 2 * lp.krad + 1;
     if (H <= lp.krad || W <= lp.krad) return fail(GT_ERR_ARG, "frame smaller than the smoothing window");
-    float norm = 0.0f;
-    for (int i = -lp.krad; i <= lp.krad; ++i) {
-        const float x = (float)i;
-        const float g = std::exp(-x * x / (2.0f * noise));
-        lp.w[i + lp.krad] = g;
-        norm = norm + g;
-    }
-    lp.norm = norm;
+    gauss_taps(k, noise, 0, lp.w, &lp.norm, &lp.rn);
     lp.kk = (float)(k * k);
+    lp.rkk = 1.0f / lp.kk;
     {
         const float v = (2.0f * (float)sep) / std::sqrt(2.0f);
         const unsigned dd = v <= 0.0f ? 0u : (unsigned)v;
@@ -217,17 +215,17 @@ extern "C" int gt_locate_frame_static(const void* d_frame, int dtype, int H, int
     lp.cpu_processed = cpu_processed;
     lp.characterize = characterize;
     lp.zero_skip = lp.max_iter >= 1 && lp.rint_c <= lp.o && lp.rint_c <= lp.D - 1 - lp.o;
+    lp.tma_spin = 1 << 22;
 
-    static float char_tab[3 * kMaxCircle], gchar_tab[2 * kMaxCircle];
-    static int char_off[2 * kMaxCircle], sig_off[2 * kMaxCircle], bg_off[2 * kMaxCircle];
+    // host staging of the stencil tables, one set per calling thread
+    thread_local float char_tab[3 * kMaxCircle], gchar_tab[2 * kMaxCircle];
+    thread_local int char_off[2 * kMaxCircle], sig_off[2 * kMaxCircle], bg_off[2 * kMaxCircle];
     lp.n_char = circle_tab(lp.char_r, char_tab, char_off, nullptr);
     lp.n_gchar = circle_tab(lp.rint_c, nullptr, nullptr, gchar_tab);
     const int n_sig = sig ? circle_f(pr->sig_radius, sig_off) : 0;
     const int n_bg = bg ? annulus_f(pr->bg_radius, pr->sig_radius + gap, bg_off) : 0;
 
-    float wmin = 1.0f;
-    for (int i = 0; i < lp.taps; ++i) wmin = std::min(wmin, lp.w[i]);
-    bool fast = dtype == GT_U16 && fast_supported(lp.krad, lp.D, lp.rint_c, lp.d) && wmin >= std::ldexp(1.0f, -40);
+    const bool fast = dtype == GT_U16 && fast_supported(lp.krad, lp.D, lp.rint_c, lp.d);
     const int th = fast ? 64 : 32;
     lp.TH = th;
     lp.TW = 64;
@@ -277,7 +275,6 @@ extern "C" int gt_locate_frame_static(const void* d_frame, int dtype, int H, int
     b.gchar_tab = d_gchar_tab;
     b.err = c.take<int>(4);
     int* off = c.take<int>(2);
-    unsigned int* dcount = c.take<unsigned int>(1);
     float* stage = c.take<float>((size_t)cap_c * ncols);
     if (c.off > kScratchBytes) return fail(GT_ERR_ARG, "parameters need more than the 16 MiB static scratch");
 
@@ -292,44 +289,9 @@ extern "C" int gt_locate_frame_static(const void* d_frame, int dtype, int H, int
     if (n_sig) SCK(cudaMemcpyAsync(d_sig_off, sig_off, sizeof(int) * 2 * n_sig, cudaMemcpyHostToDevice, st));
     if (n_bg) SCK(cudaMemcpyAsync(d_bg_off, bg_off, sizeof(int) * 2 * n_bg, cudaMemcpyHostToDevice, st));
 
-    // fixed-divisor division of the specialised kernel, verified once per
-    // divisor on this device (verify_division_kernel)
-    FixedDiv dn{1.0f / lp.norm, -lp.norm}, dk{1.0f / lp.kk, -lp.kk};
-    if (fast) {
-        const float divs[2] = {lp.norm, lp.kk};
-        const FixedDiv fdv[2] = {dn, dk};
-        for (int i = 0; i < 2 && fast; ++i) {
-            uint32_t bits;
-            std::memcpy(&bits, &divs[i], 4);
-            int slot = -1;
-            for (int q = 0; q < ds.ndiv; ++q)
-                if (ds.div_bits[q] == bits) slot = q;
-            if (slot < 0) {
-                SCK(cudaMemsetAsync(dcount, 0, sizeof(unsigned int), st));
-                SCK(launch_verify_division(divs[i], fdv[i], dcount, ds.num_sms, st));
-                unsigned int bad = 0;
-                SCK(cudaMemcpyAsync(&bad, dcount, sizeof(bad), cudaMemcpyDeviceToHost, st));
-                SCK(cudaStreamSynchronize(st));
-                if (ds.ndiv < 16) {
-                    ds.div_bits[ds.ndiv] = bits;
-                    ds.div_ok[ds.ndiv] = bad == 0;
-                    ++ds.ndiv;
-                }
-                fast = bad == 0;
-            } else {
-                fast = ds.div_ok[slot];
-            }
-        }
-        if (!fast) {  // generic kernel plan
-            lp.TH = 32;
-            lp.nty = (H + 31) / 32;
-        }
-    }
-
     if (fast) {
         int used_tma = 0;
-        SCK(launch_locate_fast(lp.krad, lp.D, lp.rint_c, 64, dim3(lp.ntx * lp.nty, 1), st, lp, b, dn, dk, 1, 0,
-                               &used_tma));
+        SCK(launch_locate_fast(lp.krad, lp.D, lp.rint_c, 64, dim3(lp.ntx * lp.nty, 1), st, lp, b, 1, 0, &used_tma));
     } else {
         const int PH = 32 + 2 * lp.hp, PW = 64 + 2 * lp.hp;
         const int RH = PH + 2 * lp.krad, RW = PW + 2 * lp.krad;
