@@ -379,7 +379,7 @@ struct Work {
     float *char_tab, *gchar_tab;
     int *char_off, *sig_off, *bg_off;
     int* err;
-    int *off, *pred, *mlist, *mcount, *dirty, *ndirty, *newrank, *newcount, *newbase, *root, *newid;
+    int *off, *pred, *mlist, *mcount, *dirty, *ndirty, *newrank, *newcount, *newbase, *root, *lroot, *newid;
     int* pbeg;  // fallback list position at the start of each chunk's locate
     unsigned long long* phase_ns;
     unsigned char* lnext;
@@ -447,6 +447,7 @@ size_t carve(const Plan& P, char* base, Work* w, size_t frame_bytes, bool need_l
     w->newcount = c.take<int>(T);
     w->newbase = c.take<int>(T + 1);
     w->root = c.take<int>(np);
+    w->lroot = c.take<int>(P.link ? np : 1);
     w->newid = c.take<int>(np);
     const size_t S = P.link ? P.nslot : 0;
     const size_t nn = (size_t)P.cap_s + P.cap_p;
@@ -499,7 +500,7 @@ LinkBufs link_bufs(const Plan& P, const Work& w, long long budget) {
     L.G = P.G; L.ncx = P.ncx; L.ncy = P.ncy;
     L.py = w.py; L.px = w.px; L.npart = w.npart; L.off = w.off; L.gstart = w.gstart; L.gidx = w.gidx;
     L.pred = w.pred; L.lnext = w.lnext; L.mlist = w.mlist; L.mcount = w.mcount; L.dirty = w.dirty;
-    L.ndirty = w.ndirty; L.newrank = w.newrank; L.newcount = w.newcount; L.root = w.root; L.err = w.err;
+    L.ndirty = w.ndirty; L.newrank = w.newrank; L.newcount = w.newcount; L.root = w.root; L.lroot = w.lroot; L.err = w.err;
     L.budget = budget;
     L.nslot = P.nslot;
     L.s_y = w.s_y; L.s_x = w.s_x; L.s_h = w.s_h; L.s_deg = w.s_deg; L.e_dst = w.e_dst; L.e_w = w.e_w;

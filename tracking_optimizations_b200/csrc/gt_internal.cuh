@@ -125,6 +125,7 @@ struct LinkBufs {
     int* newrank;         // compact: rank among new particles of its frame
     int* newcount;        // T
     int* root;            // compact
+    int* lroot;           // compact: where the pred chain enters the particle's chunk
     int* err;
     long long budget;     // branch-and-bound option trials per subnet
     // per-CTA scratch, `nslot` slots of these sizes

@@ -583,39 +583,67 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
     }
 }
 
-// Trajectory roots (the first particle of each trajectory, compact index).
-// root[] is reset to -1, then every particle walks its pred chain until it
-// meets a particle whose root is already written or a trajectory start.
-// root[] only ever receives final values, so the walks need no barrier
-// between hops and the result is exact whatever the interleaving; particles
-// of early frames finish first and shorten the later walks.
-__device__ void roots_reset(const LinkBufs& L) {
-    const int g0 = L.off[L.tb], n = L.off[L.te];
-    const int stride = gridDim.x * blockDim.x;
-    for (int g = g0 + blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) L.root[g] = -1;
+// Trajectory roots (the first particle of each trajectory, compact index),
+// in two levels.  Compact indices run in frame order and a pred always
+// points to an earlier particle, so a chain only ever steps to smaller
+// indices.  The window's particles are cut into about sqrt(frames) chunks
+// of consecutive indices:
+//   roots_local:  every particle walks its pred chain while it stays inside
+//                 its own chunk (at most the chunk's frame count of hops)
+//                 and records where the chain enters the chunk (lroot);
+//                 root[] is cleared meanwhile;
+//   roots_global: every particle steps from chunk to chunk through
+//                 lroot(pred(entry)) until a trajectory start, a particle of
+//                 an earlier (final) window, or a root another thread has
+//                 written -- at most the chunk count of hops.
+// root[] only ever receives final values, so no barrier is needed between
+// hops; a chain costs O(sqrt(frames)) dependent loads instead of O(frames).
+__device__ __forceinline__ int root_chunk(const LinkBufs& L) {
+    const int n = L.off[L.te] - L.off[L.tb];
+    int nc = 1;
+    while (nc * nc < L.te - L.tb) ++nc;
+    return max(1, (n + nc - 1) / nc);
 }
 
-__device__ void roots_walk(const LinkBufs& L) {
+__device__ void roots_local(const LinkBufs& L) {
+    const int g0 = L.off[L.tb], n = L.off[L.te];
+    const int cs = root_chunk(L);
+    const int stride = gridDim.x * blockDim.x;
+    for (int g = g0 + blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) {
+        const int cbeg = g0 + (g - g0) / cs * cs;
+        int r = g;
+        while (true) {
+            const int p = __ldcg(L.pred + r);
+            if (p < cbeg) break;
+            r = p;
+        }
+        L.lroot[g] = r;
+        L.root[g] = -1;
+    }
+}
+
+__device__ void roots_global(const LinkBufs& L) {
     const int g0 = L.off[L.tb], n = L.off[L.te];
     const int stride = gridDim.x * blockDim.x;
     volatile int* root = L.root;
     for (int g = g0 + blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) {
-        int r = g;
+        int r = __ldcg(L.lroot + g);
         while (true) {
             const int known = root[r];
             if (known >= 0) { r = known; break; }
             const int p = __ldcg(L.pred + r);
             if (p < 0) break;
-            r = p;
+            if (p < g0) { r = root[p]; break; }  // earlier window: final
+            r = __ldcg(L.lroot + p);
         }
         root[g] = r;
     }
 }
 
 __device__ void roots_body(const LinkBufs& L, cg::grid_group& grid) {
-    roots_reset(L);
+    roots_local(L);
     grid.sync();
-    roots_walk(L);
+    roots_global(L);
 }
 
 // The whole linker in one cooperative launch: link every frame with M = {},
@@ -695,10 +723,10 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_multi_kernel(const LinkB
         for (k = 1; k <= max_passes; ++k) {
             grid.sync();
             for (int m = 0; m < nm; ++m)
-                if (active(m, k)) roots_reset(Ls[m]);
+                if (active(m, k)) roots_local(Ls[m]);
             grid.sync();
             for (int m = 0; m < nm; ++m)
-                if (active(m, k)) roots_walk(Ls[m]);
+                if (active(m, k)) roots_global(Ls[m]);
             grid.sync();
             for (int m = 0; m < nm; ++m)
                 if (active(m, k)) memory_body(Ls[m], memory[m], ndirty + k * nm + m, t0_of(m), G);
@@ -711,9 +739,9 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_multi_kernel(const LinkB
         }
     }
     grid.sync();
-    for (int m = 0; m < nm; ++m) roots_reset(Ls[m]);
+    for (int m = 0; m < nm; ++m) roots_local(Ls[m]);
     grid.sync();
-    for (int m = 0; m < nm; ++m) roots_walk(Ls[m]);
+    for (int m = 0; m < nm; ++m) roots_global(Ls[m]);
     if (blockIdx.x == 0 && threadIdx.x == 0) *passes = k;
 }
 

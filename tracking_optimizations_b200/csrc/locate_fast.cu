@@ -88,7 +88,7 @@ struct Geo {
     static constexpr int SZ_GP = align128(cmax(cmax(RPA * GPS * 8, (PP + 1) * RMS * 8), TH0 * FT * 4));
     static constexpr int SZ_BP = align128(cmax(RPA * GPS * 8, TH0 * FT));
     static constexpr int K = circle_size(RC);
-    static constexpr int SZ_TAB = align128(K * 8);
+    static constexpr int SZ_TAB = align128(K * 20);  // (sin2, cos2), P2 offsets by parity, r2
     static constexpr int OFF_GP = SZ_P2;
     static constexpr int OFF_BP = OFF_GP + SZ_GP;
     static constexpr int OFF_U = OFF_BP + SZ_BP;
@@ -108,6 +108,7 @@ struct Geo {
     static_assert((NPW - 1) * FM < US && (FM * 2) % 16 == 0, "16-byte raw loads start inside a U row");
     static_assert(SMEM <= 227 * 1024, "shared memory");
     static_assert(RC + 2 <= HP && RC <= HX, "walk and feature circles inside the processed region");
+    static_assert(TH0 * FT + (fast_threads(TH0) / 32) * 32 * 20 <= SZ_BP, "emission staging fits the dead boxcar region");
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -144,6 +145,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
+// max(a, b, c) in one instruction (sm_100 three-input max.f32)
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // max over v[m .. m+DD-1] for m = 0..M-1, sharing the common core
 template <int DD, int M>
 __device__ __forceinline__ void slide_max(const float (&v)[M + DD - 1], float (&out)[M]) {
@@ -151,14 +159,19 @@ __device__ __forceinline__ void slide_max(const float (&v)[M + DD - 1], float (&
 #pragma unroll
         for (int m = 0; m < M; ++m) {
             float x = v[m];
+            int j = 1;
 #pragma unroll
-            for (int j = 1; j < DD; ++j) x = fmaxf(x, v[m + j]);
+            for (; j + 1 < DD; j += 2) x = fmax3(x, v[m + j], v[m + j + 1]);
+            if (j < DD) x = fmaxf(x, v[m + j]);
             out[m] = x;
         }
     } else {
+        // core = max(v[M-1 .. DD-1])
         float core = v[M - 1];
+        int j = M;
 #pragma unroll
-        for (int j = M; j < DD; ++j) core = fmaxf(core, v[j]);
+        for (; j + 1 < DD; j += 2) core = fmax3(core, v[j], v[j + 1]);
+        if (j < DD) core = fmaxf(core, v[j]);
         float suf[M];  // suf[m] = max(v[m .. M-2]), m <= M-2
         suf[M - 1] = -CUDART_INF_F;
 #pragma unroll
@@ -167,7 +180,7 @@ __device__ __forceinline__ void slide_max(const float (&v)[M + DD - 1], float (&
 #pragma unroll
         for (int m = 0; m < M; ++m) {
             if (m > 0) pre = fmaxf(pre, v[DD + m - 1]);
-            out[m] = fmaxf(fmaxf(suf[m], core), pre);
+            out[m] = fmax3(suf[m], core, pre);
         }
     }
 }
@@ -210,55 +223,65 @@ __device__ __forceinline__ void circle_centroid(const float* P, int base, float&
     }
 }
 
-// eight-lane fold of ndarray's unrolled_fold: acc = 0 + (p0+p4) + (p1+p5) + ...
-__device__ __forceinline__ float fold8(const float (&a)[8]) {
-    float acc = 0.f;
-    acc = acc + (a[0] + a[4]);
-    acc = acc + (a[1] + a[5]);
-    acc = acc + (a[2] + a[6]);
-    acc = acc + (a[3] + a[7]);
-    return acc;
-}
-
 // cpu_processed sums of processed * {r2, sin2, cos2} over the d/2 circle
-// (equal to the centroid circle for odd d), products folded as ndarray's
-// sum_axis does (execute_gpu.rs:289-291), fully unrolled.
-template <int RC, int E, int S>
-__device__ __forceinline__ void circle_features(const float* P, int base, const float2* sc, float& rg, float& sn,
-                                                float& cs, float& sig) {
+// (equal to the centroid circle for odd d), folded as ndarray's sum_axis
+// does (execute_gpu.rs:289-291: eight interleaved accumulators, combined
+// (p0+p4), (p1+p5), (p2+p6), (p3+p7) into 0 in that order, then the
+// leftover elements in order), and the maximum (signal), computed by the 8
+// lanes of a lane group (l = lane & 7,
+// groups of 8 consecutive lanes share one record): lane l accumulates the
+// products of circle elements l, l + 8, l + 16, ... (accumulator l), the
+// group folds them, and group lane 0 adds the leftover elements.  offs
+// holds each element's P2 offset for a centre row of parity 0 (.x) and 1
+// (.y).  Every lane of the warp must call it; results on group lane 0.
+template <int RC>
+__device__ __forceinline__ void circle_features_group(const float* P, int base, int E, const int2* offs,
+                                                      const float* r2, const float2* sc, int l, float& rg,
+                                                      float& sn, float& cs, float& sig) {
     constexpr int K = circle_size(RC);
     constexpr int K8 = K & ~7;
-    float ar[8], as[8], ac[8];
+    const unsigned full = 0xffffffffu;
+    float pr = 0.f, ps = 0.f, pc = 0.f, mx = -CUDART_INF_F;
 #pragma unroll
-    for (int l = 0; l < 8; ++l) { ar[l] = 0.f; as[l] = 0.f; ac[l] = 0.f; }
-    float tr = 0.f, ts = 0.f, tc = 0.f;
-    sig = -CUDART_INF_F;
-    int q = 0;
-#pragma unroll
-    for (int i = -RC; i <= RC; ++i) {
-#pragma unroll
-        for (int j = -RC; j <= RC; ++j) {
-            if (i * i + j * j > RC * RC) continue;
-            const float nb = P[base + ((((E + i) >> 1) * S + j) << 1) + ((E + i) & 1)];
-            const float2 t = sc[q];
-            const float pr = nb * (float)(i * i + j * j), ps = nb * t.x, pc = nb * t.y;
-            sig = fmaxf(sig, nb);
-            if (q < K8) {
-                ar[q & 7] = ar[q & 7] + pr;
-                as[q & 7] = as[q & 7] + ps;
-                ac[q & 7] = ac[q & 7] + pc;
-                if (q == K8 - 1) { tr = fold8(ar); ts = fold8(as); tc = fold8(ac); }
-            } else {
-                tr = tr + pr;
-                ts = ts + ps;
-                tc = tc + pc;
-            }
-            ++q;
-        }
+    for (int q0 = 0; q0 < K8; q0 += 8) {
+        const int q = q0 + l;
+        const int2 o = offs[q];
+        const float nb = P[base + (E ? o.y : o.x)];
+        const float2 t = sc[q];
+        pr = pr + nb * r2[q];
+        ps = ps + nb * t.x;
+        pc = pc + nb * t.y;
+        mx = fmaxf(mx, nb);
     }
-    rg = tr;
-    sn = ts;
-    cs = tc;
+    // (p_l + p_{l+4}) on lanes l < 4 of the group
+    const float qr = pr + __shfl_down_sync(full, pr, 4);
+    const float qs = ps + __shfl_down_sync(full, ps, 4);
+    const float qc = pc + __shfl_down_sync(full, pc, 4);
+    float ar = 0.f, as = 0.f, ac = 0.f;
+    ar = ar + qr; as = as + qs; ac = ac + qc;
+#pragma unroll
+    for (int k = 1; k < 4; ++k) {
+        ar = ar + __shfl_down_sync(full, qr, k);
+        as = as + __shfl_down_sync(full, qs, k);
+        ac = ac + __shfl_down_sync(full, qc, k);
+    }
+    mx = fmaxf(mx, __shfl_xor_sync(full, mx, 1));
+    mx = fmaxf(mx, __shfl_xor_sync(full, mx, 2));
+    mx = fmaxf(mx, __shfl_xor_sync(full, mx, 4));
+#pragma unroll
+    for (int q = K8; q < K; ++q) {  // leftover elements, in order
+        const int2 o = offs[q];
+        const float nb = P[base + (E ? o.y : o.x)];
+        const float2 t = sc[q];
+        ar = ar + nb * r2[q];
+        as = as + nb * t.x;
+        ac = ac + nb * t.y;
+        mx = fmaxf(mx, nb);
+    }
+    rg = ar;
+    sn = as;
+    cs = ac;
+    sig = mx;
 }
 
 template <class G, int RC>
@@ -353,9 +376,16 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     }
     if (tid < TH0) rowmask[tid] = 0ull;
     if (tid == 0) s_nc = 0;
+    int2* offs = (int2*)(smem + G::OFF_TAB + G::K * 8);  // P2 offsets of the d/2 circle by centre parity
+    float* r2s = (float*)(smem + G::OFF_TAB + G::K * 16);
     if (p.cpu_processed)
-        for (int k = tid; k < G::K; k += NTK)
+        for (int k = tid; k < G::K; k += NTK) {
             sc[k] = make_float2(__ldg(b.char_tab + 3 * k + 1), __ldg(b.char_tab + 3 * k + 2));
+            r2s[k] = __ldg(b.char_tab + 3 * k);
+            const int di = __ldg(b.char_off + 2 * k), dj = __ldg(b.char_off + 2 * k + 1);
+            offs[k] = make_int2(((di >> 1) * G::P2S + dj) * 2 + (di & 1),
+                                (((1 + di) >> 1) * G::P2S + dj) * 2 + ((1 + di) & 1));
+        }
 
     float2 W2[TAPS];
 #pragma unroll
@@ -446,12 +476,20 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             for (int k = 0; k < FM / 2 + KR; ++k) L[k] = Bp[(p0 + k) * G::GPS + c];
 #pragma unroll
             for (int k = 0; k < FM / 2 + KR - 1; ++k) ML[k] = make_float2(L[k].y, L[k + 1].x);
+            // the first window summed in tap order, the next ones slid by
+            // one row pair; every partial sum is an integer below 2^24
+            // (u16 frames), so all orders give the same bits
+            {
+                float2 s = L[0];
 #pragma unroll
-            for (int m = 0; m < FM / 2; ++m) {
-                float2 s = L[m];
+                for (int j = 1; j < TAPS; ++j) s = add2(s, (j & 1) ? ML[j >> 1] : L[j >> 1]);
+                cs[0] = s;
 #pragma unroll
-                for (int j = 1; j < TAPS; ++j) s = add2(s, (j & 1) ? ML[m + (j >> 1)] : L[m + (j >> 1)]);
-                cs[m] = s;
+                for (int m = 0; m + 1 < FM / 2; ++m) {
+                    s = add2(add2(s, L[m + 1 + KR]), ML[m + KR]);
+                    s = sub2(sub2(s, L[m]), ML[m]);
+                    cs[m + 1] = s;
+                }
             }
         } else {
             // reflect-padded boxcar at the top/bottom frame edges
@@ -646,10 +684,15 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = __popcll(rowmask[r]);
 
     // emission: the first stride of the list from the walks above, later
-    // strides as pending records
+    // strides as pending records.  The cpu_processed sums of a stride's
+    // records are computed by lane groups of 8, four records at a time
+    // (circle_features_group); the slot atomic issued above completes
+    // meanwhile.
     const unsigned short* frame = (const unsigned short*)b.frames + (size_t)t * H * W;
     GRawAcc racc{frame, W};
-    gbase = __shfl_sync(0xffffffffu, gbase, 0);
+    const float* P2f = (const float*)P2;
+    int* stage = (int*)((unsigned char*)Bp + TH0 * FT) + warp * 32;  // flags are dead here
+    float4* sfeat = (float4*)((unsigned char*)Bp + TH0 * FT + NW * 32 * 4) + warp * 32;
     int roff = 0;
     for (int c0 = 0; c0 < ncand; c0 += wstride) {
         int rq = q, rtr = tr, rtc = tc, rst = st;
@@ -666,8 +709,30 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         }
         const bool em = rst != CAND_REJECT;
         const unsigned eb = __ballot_sync(0xffffffffu, em);
+        const int ne = __popc(eb), e = __popc(eb & lt);
+        const int ru = ty0 + rtr, rv = tx0 + rtc;
+        float4 feat = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (p.cpu_processed && ne) {
+            // execute_gpu.rs:165-172, 286-299 at the originating pixel
+            if (em) stage[e] = ((ru - py0) << 16) | (rv - px0);
+            __syncwarp();
+            for (int g = 0; g < ne; g += 4) {
+                const int er = min(g + (lane >> 3), ne - 1);
+                const int code = stage[er];
+                const int rr = code >> 16, cc = code & 0xffff;
+                float a0, a1, a2, a3;
+                circle_features_group<RC>(P2f, ((rr >> 1) * G::P2S + cc) * 2, rr & 1, offs, r2s, sc, lane & 7,
+                                          a0, a1, a2, a3);
+                if ((lane & 7) == 0 && g + (lane >> 3) < ne) sfeat[g + (lane >> 3)] = make_float4(a0, a1, a2, a3);
+            }
+            __syncwarp();
+            if (em) feat = sfeat[e];
+            __syncwarp();  // stage and sfeat are reused by the next stride
+        }
+        // the slot base of lane 0's atomic, read only now: its latency
+        // overlapped the sums above
+        const int gb = __shfl_sync(0xffffffffu, gbase, 0);
         if (em) {
-            const int ru = ty0 + rtr, rv = tx0 + rtc;
             Cand rec;
             rec.u = ru; rec.v = rv;
             rec.y = ry; rec.x = rx; rec.mass = rm;
@@ -679,20 +744,14 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             rec.up = (int)(rfp >> 16); rec.vp = (int)(rfp & 0xffffu);
             rec.pad = 0;
             if (p.cpu_processed) {
-                // execute_gpu.rs:165-172, 286-299 at the originating pixel
-                const int rr = ru - py0, cc = rv - px0;
-                const int base2 = (((rr >> 1) * G::P2S + cc) << 1);
-                float rg, sn, cs2, sig;
-                if (rr & 1) circle_features<RC, 1, G::P2S>((const float*)P2, base2, sc, rg, sn, cs2, sig);
-                else circle_features<RC, 0, G::P2S>((const float*)P2, base2, sc, rg, sn, cs2, sig);
-                rec.rg_sum = rg;
-                rec.eccn = sqrtf(sn * sn + cs2 * cs2);
+                rec.rg_sum = feat.x;
+                rec.eccn = sqrtf(feat.y * feat.y + feat.z * feat.z);
                 rec.mid = acc(ru, rv);
-                rec.signal = sig;
+                rec.signal = feat.w;
             }
             if (p.characterize) gpu_features(p, b, acc, racc, ru, rv, rec);
-            if (gbase >= 0) {
-                const int slot = gbase + roff + __popc(eb & lt);
+            if (gb >= 0) {
+                const int slot = gb + roff + e;
                 b.cand[(size_t)t * b.cap_c + slot] = rec;
                 if (rec.state == CAND_PENDING) {
                     const int k = atomicAdd(b.npend, 1);
@@ -700,7 +759,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
                 }
             }
         }
-        roff += __popc(eb);
+        roff += ne;
     }
 }
 
