@@ -9,7 +9,7 @@ search_range 5, memory 2, cpu_processed=True.  A step = locate + link of the
 whole movie.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--workload locate-link|adjoint|batched|file|postprocess]
+                  [--workload locate-link|adjoint|batched|file|postprocess|dense-link]
 
 The other workloads print one line each: the adjoint of bandpass + refine
 at fixed peaks (256 x 512x512 f32), 64 uneven movies in one graph launch
@@ -488,6 +488,65 @@ def run_file(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
+def run_dense(args, rank, world, local):
+    """--workload dense-link: the dense linking stress movie (200 frames of
+    2048x2048 u16, 20,000 spots per frame, sigma 1.5, Brownian 2.5 px,
+    diameter 9, search_range 7, memory 3), rendered on the device; one step
+    = one gt_batch_device call (locate + link); the line reports the
+    linker's share and its fixed-point passes."""
+    import torch
+
+    from tracking_optimizations_b200 import _native, synth
+
+    torch.cuda.set_device(local)
+    spec = synth.scaled(synth.DENSE_LINK, frames=args.frames or synth.DENSE_LINK.frames,
+                        seed=synth.DENSE_LINK.seed + rank)
+    params = dict(spec.params)
+    fr = synth.make_movie_device(spec, f"cuda:{local}")
+    T, H, W = fr.shape
+    lib = _native.load()
+    ctx = _native.context(local)
+    gp = _native.make_params(**params)
+    out = torch.empty((T * 30000, 5), dtype=torch.float32, device=f"cuda:{local}")
+    nrows = ctypes.c_int64()
+    stream = torch.cuda.current_stream()
+
+    def step():
+        _native.check(lib.gt_batch_device(ctx, ctypes.c_void_p(fr.data_ptr()), _native.GT_U16, T, H, W,
+                                          ctypes.byref(gp), ctypes.c_void_p(out.data_ptr()), out.shape[0],
+                                          ctypes.byref(nrows), ctypes.c_void_p(stream.cuda_stream)), ctx)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    stats = []
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        stats.append(_native.last_stats(local))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world, f"cuda:{local}")
+    if rank != 0:
+        return
+    med = lambda k: float(np.median([s_[k] for s_ in stats]))  # noqa: E731
+    line = {
+        "metric": "dense linking stress: locate+link frames/s at 2048^2 x 200 u16, 20000 spots/frame",
+        "value": aggregate_rate(T, world, ms), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(1, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16 in / f32 compute", "data": "synthetic (device renderer)",
+        "config": {"workload": f"dense linking stress: {T} frames x {H}x{W} u16, {spec.spots} spots/frame, "
+                               "step 2.5 px", "params": params},
+        "stages_ms": {k: med(k) for k in ["ms_locate", "ms_finalize", "ms_link", "ms_assemble", "ms_total"]},
+        "link_iterations": stats[-1]["link_iterations"],
+        "link_phase_ms": {k: float(np.median([s_["link_phase_ms"][i] for s_ in stats]))
+                          for i, k in enumerate(["first", "roots", "memory", "relink"])},
+        "rows": int(nrows.value),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_postprocess(args, rank, world, local):
     """--workload postprocess: the lab pipeline's steps after linking
     (all_cleaned_up/hatzakis_lab_tracking.py:216-232: filter_stubs,
@@ -577,7 +636,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="locate-link", choices=["locate-link", "adjoint", "batched", "file",
-                                                                     "postprocess"])
+                                                                     "postprocess", "dense-link"])
     ap.add_argument("--frames", type=int, default=None,
                     help="smaller movie of the same spot model (profiling captures only)")
     args = ap.parse_args()
@@ -595,6 +654,9 @@ def main():
         return
     if args.workload == "file":
         run_file(args, rank, world, local)
+        return
+    if args.workload == "dense-link":
+        run_dense(args, rank, world, local)
         return
     if args.workload == "postprocess":
         run_postprocess(args, rank, world, local)
@@ -674,9 +736,10 @@ def main():
         loc_ms = float(np.median([s["ms_locate"] for s in stats]))
         cands = stats[-1]["candidates"]
         rows = stats[-1]["particles"]
-        # algorithmic bytes of one locate launch: frames read once (u16) +
-        # candidate records written (80 B each)
-        loc_bytes = T * H * W * 2 + cands * 80
+        # algorithmic bytes of the path per step: frames read once (u16) +
+        # the output table (rows x columns x 4 B) + the previous frame's
+        # table re-read by the linker (y, x, id: 12 B per particle)
+        loc_bytes = T * H * W * 2 + rows * ncols * 4 + rows * 12
         peak, kind = peaks()
         achieved = loc_bytes / (loc_ms / 1e3) / 1e9
         traffic = locate_traffic(T)
@@ -692,6 +755,8 @@ def main():
             "stages_ms": {k: float(np.median([s[k] for s in stats]))
                           for k in ["ms_locate", "ms_finalize", "ms_link", "ms_assemble", "ms_total"]},
             "link_iterations": stats[-1]["link_iterations"], "fallback_walks": stats[-1]["fallback_walks"],
+            "link_phase_ms": {k: float(np.median([s["link_phase_ms"][i] for s in stats]))
+                              for i, k in enumerate(["first", "roots", "memory", "relink"])},
             "candidates_per_frame": cands / T, "particles_per_frame": rows / T,
             "gpu_launches": int(sum(s["launches"] for s in stats)),
             "e2e": None if e2e_value is None else {

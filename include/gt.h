@@ -183,8 +183,10 @@ GT_API int gt_adjoint_forward(gt_ctx* ctx, const float* d_frames, int T, int H, 
  * dL/dsmoothing_size.  The clip of the bandpass at 0 takes subgradient 0;
  * smoothing_size is differentiated through the box normalisation 1/k^2
  * treated as continuous in k (window and Gaussian taps held fixed).
- * Gradients are summed with atomic additions: bitwise run-to-run equality
- * is not guaranteed where particle circles overlap. */
+ * d_grad_params is reduced in a fixed order (per-block partials, then one
+ * ordered pass) and is the same on every run; d_grad_frames is summed with
+ * atomic additions where particle circles overlap, so those pixels may
+ * differ in the last bits from run to run. */
 GT_API int gt_adjoint_backward(gt_ctx* ctx, const float* d_frames, int T, int H, int W,
                         const gt_params* params, const int32_t* d_walk, int64_t n,
                         const float* d_grad_yxm, float* d_grad_frames,

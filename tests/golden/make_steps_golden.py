@@ -8,7 +8,7 @@ module (by its syntax tree) and executed with numpy and pandas -- the code
 that runs is the reference's, unchanged.  Run once where the reference tree
 is present:
 
-    python tests/golden/make_steps_golden.py /root/reference
+    REFERENCE_ROOT=<path to the reference checkout> python tests/golden/make_steps_golden.py
 
 The table: 60 frames, particle ids interleaved within each frame (so that
 step_tracker's positional assignment of its groupby-ordered lists is visible),
@@ -73,4 +73,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref_root = os.environ.get("REFERENCE_ROOT") or (sys.argv[1] if len(sys.argv) > 1 else None)
+    if not ref_root:
+        sys.exit("set REFERENCE_ROOT (or pass the reference checkout as the first argument)")
+    main(ref_root)

@@ -191,19 +191,27 @@ def uncertainty(frames, walk, diameter, gain=1.0, read_noise=0.0, **params):
     return out
 
 
-def calibrate_noise_size(frames, walk, target_yx, diameter, noise_size=1.0, steps=50, lr=0.05, **params):
+def calibrate_noise_size(frames, walk, target_yx, diameter, noise_size=1.0, steps=50, lr=0.05, lr_min_frac=0.1,
+                         **params):
     """Fit ``noise_size`` so that the refined positions of ``walk`` approach
     ``target_yx`` ((n, 2), e.g. simulated ground truth): Adam on the mean
     squared position error through RefineAtPeaks.  The Gaussian variance is
-    optimised in log space so that it stays positive.  Returns
-    ``(noise_size, losses)`` with one loss per step (before the update)."""
+    optimised in log space so that it stays positive; the learning rate
+    decays from ``lr`` to ``lr * lr_min_frac`` on a cosine schedule.
+    Returns ``(noise_size, losses)`` with one loss per step (before the
+    update).  The parameter gradient is reduced in a fixed order, so the
+    same inputs give the same trajectory."""
+    import math
+
     dev = frames.device
     target = target_yx.to(device=dev, dtype=torch.float32)
     log_s = torch.tensor(float(noise_size), dtype=torch.float64, device=dev).log().requires_grad_(True)
     ks = torch.tensor(float(params.pop("smoothing_size", diameter)), dtype=torch.float64, device=dev)
     opt = torch.optim.Adam([log_s], lr=lr)
     losses = []
-    for _ in range(steps):
+    for i in range(steps):
+        for g in opt.param_groups:
+            g["lr"] = lr * (lr_min_frac + (1.0 - lr_min_frac) * 0.5 * (1.0 + math.cos(math.pi * i / steps)))
         opt.zero_grad()
         yxm = refine(frames, walk, diameter, noise_size=log_s.exp(), smoothing_size=ks, **params)
         loss = ((yxm[:, :2] - target) ** 2).sum(dim=1).mean()

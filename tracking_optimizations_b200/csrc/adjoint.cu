@@ -249,17 +249,44 @@ __global__ void __launch_bounds__(ADJ_NT) adjoint_particle_kernel(AdjParams p, c
         }
     }
     if constexpr (MODE == ADJ_BACKWARD) {
-        // one atomic pair per block instead of one per particle (all
-        // particles add to the same two words)
+        // this block's partial sums, in warp order; adjoint_param_reduce_kernel
+        // adds the blocks' partials in block order, so the parameter
+        // gradient is the same on every run (particles map to warps and
+        // blocks by a fixed grid stride)
         __shared__ double red[2 * NW];
         if (lane == 0) { red[2 * wid] = acc_ds; red[2 * wid + 1] = acc_dk; }
         __syncthreads();
         if (threadIdx.x == 0) {
             double a = 0.0, c = 0.0;
             for (int w = 0; w < NW; ++w) { a += red[2 * w]; c += red[2 * w + 1]; }
-            atomicAdd(gpar, a);
-            atomicAdd(gpar + 1, c);
+            gpar[2 * blockIdx.x] = a;
+            gpar[2 * blockIdx.x + 1] = c;
         }
+    }
+}
+
+// out[0..1] = the sums of part[2b], part[2b + 1] over blocks b in a fixed
+// order: thread i takes blocks i, i + 256, ... in order, then a fixed tree.
+__global__ void __launch_bounds__(256) adjoint_param_reduce_kernel(const double* part, int nblocks, double* out) {
+    __shared__ double sa[256], sc[256];
+    double a = 0.0, c = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += 256) {
+        a += part[2 * b];
+        c += part[2 * b + 1];
+    }
+    sa[threadIdx.x] = a;
+    sc[threadIdx.x] = c;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            sa[threadIdx.x] += sa[threadIdx.x + h];
+            sc[threadIdx.x] += sc[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sa[0];
+        out[1] = sc[0];
     }
 }
 
@@ -395,9 +422,13 @@ size_t adjoint_transpose_smem(int kr) {
     return sizeof(float) * (size_t)(SH * SW + 2 * SH * (TR_TW + 1));
 }
 
+// Upper bound of the particle kernel's grid (partial sums of the backward
+// pass: two doubles per block).
+int adjoint_particle_blocks_max(int num_sms) { return num_sms * 16; }
+
 cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* frames, const int* walk, long long n,
                                      const int* circ, const float* grad, float* yxm, float* gR, double* gpar,
-                                     int* err, int num_sms, cudaStream_t st) {
+                                     double* gpart, int* err, int num_sms, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const size_t smem = adjoint_particle_smem(p.K);
     const int grid = (int)std::min<long long>((n + ADJ_NT / 32 - 1) / (ADJ_NT / 32), (long long)num_sms * 16);
@@ -415,7 +446,10 @@ cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* 
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e) return e;
             adjoint_particle_kernel<ADJ_BACKWARD><<<grid, ADJ_NT, smem, st>>>(p, frames, walk, n, circ, grad, yxm,
-                                                                              gR, gpar, err);
+                                                                              gR, gpart, err);
+            e = cudaGetLastError();
+            if (e) return e;
+            adjoint_param_reduce_kernel<<<1, 256, 0, st>>>(gpart, grid, gpar);
             break;
         default:
             e = cudaFuncSetAttribute(adjoint_particle_kernel<ADJ_UNCERTAINTY>,

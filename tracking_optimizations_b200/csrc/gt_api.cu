@@ -45,7 +45,8 @@ cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaSt
 void gauss_taps(int smoothing_size, float noise_size, int normalized, float* w, float* norm, float* rn);
 cudaError_t launch_adjoint_particles(int mode, const AdjParams& p, const float* frames, const int* walk, long long n,
                                      const int* circ, const float* grad, float* yxm, float* gR, double* gpar,
-                                     int* err, int num_sms, cudaStream_t st);
+                                     double* gpart, int* err, int num_sms, cudaStream_t st);
+int adjoint_particle_blocks_max(int num_sms);
 cudaError_t launch_adjoint_transpose(const AdjParams& p, const float* gR, float* gI, cudaStream_t st);
 __global__ void link_fixpoint_multi_kernel(const LinkBufs* Ls, const int* memory, const int* fstart, int nm,
                                            int max_passes, int* ndirty, int* passes);
@@ -1581,17 +1582,21 @@ struct AdjWork {
     int* err;
     int* circ;
     float* plane;
+    double* gpart;  // per-block partial parameter gradients (backward only)
 };
 
 int adjoint_work(gt_ctx* ctx, const AdjParams& ap, const std::vector<int>& circ, bool plane, AdjWork* aw,
                  cudaStream_t st) {
     const size_t off_circ = 256;
-    const size_t off_plane = off_circ + ((sizeof(int) * circ.size() + 255) / 256) * 256;
+    const size_t off_part = off_circ + ((sizeof(int) * circ.size() + 255) / 256) * 256;
+    const size_t n_part = 2 * (size_t)adjoint_particle_blocks_max(ctx->num_sms);
+    const size_t off_plane = off_part + ((sizeof(double) * n_part + 255) / 256) * 256;
     const size_t need = off_plane + (plane ? sizeof(float) * (size_t)ap.T * ap.H * ap.W : 0);
     int rc = ensure_arena(ctx, need);
     if (rc) return rc;
     aw->err = (int*)ctx->arena;
     aw->circ = (int*)(ctx->arena + off_circ);
+    aw->gpart = (double*)(ctx->arena + off_part);
     aw->plane = plane ? (float*)(ctx->arena + off_plane) : nullptr;
     CK(cudaMemsetAsync(aw->err, 0, sizeof(int), st));
     CK(cudaMemcpyAsync(aw->circ, circ.data(), sizeof(int) * circ.size(), cudaMemcpyHostToDevice, st));
@@ -1828,7 +1833,7 @@ int gt_adjoint_forward(gt_ctx* ctx, const float* d_frames, int T, int H, int W, 
     rc = adjoint_work(ctx, ap, circ, false, &aw, st);
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[0], st));
-    CK(launch_adjoint_particles(0, ap, d_frames, d_walk, n, aw.circ, nullptr, d_yxm, nullptr, nullptr, aw.err,
+    CK(launch_adjoint_particles(0, ap, d_frames, d_walk, n, aw.circ, nullptr, d_yxm, nullptr, nullptr, nullptr, aw.err,
                                 ctx->num_sms, st));
     CK(cudaEventRecord(ctx->ev[1], st));
     ctx->stats.launches = n > 0 ? 1 : 0;
@@ -1850,15 +1855,15 @@ int gt_adjoint_backward(gt_ctx* ctx, const float* d_frames, int T, int H, int W,
     AdjWork aw;
     rc = adjoint_work(ctx, ap, circ, true, &aw, st);
     if (rc) return rc;
-    CK(cudaMemsetAsync(d_grad_params, 0, 2 * sizeof(double), st));
+    if (n == 0) CK(cudaMemsetAsync(d_grad_params, 0, 2 * sizeof(double), st));
     CK(cudaEventRecord(ctx->ev[0], st));
     CK(cudaMemsetAsync(aw.plane, 0, sizeof(float) * (size_t)T * H * W, st));
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(launch_adjoint_particles(1, ap, d_frames, d_walk, n, aw.circ, d_grad_yxm, nullptr, aw.plane, d_grad_params,
-                                aw.err, ctx->num_sms, st));
+                                aw.gpart, aw.err, ctx->num_sms, st));
     CK(cudaEventRecord(ctx->ev[2], st));
     CK(launch_adjoint_transpose(ap, aw.plane, d_grad_frames, st));
-    ctx->stats.launches = (n > 0 ? 1 : 0) + (T + 65534) / 65535;
+    ctx->stats.launches = (n > 0 ? 2 : 0) + (T + 65534) / 65535;
     // the dense part is the zeroing plus the transposed bandpass
     if (!ctx->ev[3]) CK(cudaEventCreate(&ctx->ev[3]));
     CK(cudaEventRecord(ctx->ev[3], st));
@@ -1891,7 +1896,7 @@ int gt_adjoint_uncertainty(gt_ctx* ctx, const float* d_frames, int T, int H, int
     rc = adjoint_work(ctx, ap, circ, false, &aw, st);
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[0], st));
-    CK(launch_adjoint_particles(2, ap, d_frames, d_walk, n, aw.circ, nullptr, d_sd, nullptr, nullptr, aw.err,
+    CK(launch_adjoint_particles(2, ap, d_frames, d_walk, n, aw.circ, nullptr, d_sd, nullptr, nullptr, nullptr, aw.err,
                                 ctx->num_sms, st));
     CK(cudaEventRecord(ctx->ev[1], st));
     ctx->stats.launches = n > 0 ? 1 : 0;
