@@ -30,8 +30,8 @@ namespace gt {
 __global__ void locate_tiles_kernel(const LocParams p, const MovieBufs b, int frame0);
 __global__ void fallback_walk_kernel(const LocParams p, const MovieBufs b, int win, const int* pbeg);
 __global__ void finalize_kernel(const LocParams p, MovieBufs b, float sep, int link_grid, int frame0);
-__global__ void link_fixpoint_kernel(LinkBufs L, int memory, int max_passes, int rounds, int* ndirty,
-                                     int* passes, unsigned long long* phase_ns);
+cudaError_t link_fixpoint_occupancy(int nt, int smem, int* per_sm);
+cudaError_t launch_link_fixpoint(int nt, int grid, void** args, int smem, cudaStream_t st);
 __global__ void scan_frames_kernel(const int* in, int* out, int n);
 __global__ void scan_frames_from_kernel(const int* in, int* out, int f0, int n);
 __global__ void newid_kernel(const int* newrank, const int* newbase, const int* off, const int* npart,
@@ -108,7 +108,8 @@ struct gt_ctx {
     cudaEvent_t bev[20] = {};         // fork/join events
     int* h_status = nullptr;          // pinned: 8 ints per movie
     int* h_stage = nullptr;           // pinned: one call's statistics, read back in one go
-    int link_per_sm = 0;              // resident link_fixpoint_kernel blocks per SM (queried once)
+    int link_per_sm = 0;              // resident link_fixpoint_kernel<256> blocks per SM (queried once)
+    int link_per_sm_big = 0;          // the same for link_fixpoint_kernel<1024>
     size_t h_stage_n = 0;
     uint16_t* h_frames = nullptr;     // pinned: decoded file frames
     size_t h_frames_n = 0;
@@ -130,6 +131,11 @@ constexpr long long SUBNET_BUDGET = 1LL << 26;  // option trials per subnet
 // that one round of blocks covers ~600 frames; frames whose data does not
 // fit use the block's global scratch slot
 constexpr int LINK_POOL_BYTES = 48 * 1024;
+// frames of at least this many pixels are linked by 1024-thread blocks (one
+// per SM, a larger shared-memory pool): their linking is latency-bound on
+// global scratch, and 32 warps per frame hide four times more of it
+constexpr long long LINK_BIG_PIXELS = 1LL << 20;
+constexpr int LINK_POOL_BYTES_BIG = 160 * 1024;
 constexpr int LINK_WINDOWS = 16;  // upload chunks of the host-frames path, at most
 
 struct Resolved {
@@ -533,28 +539,40 @@ int link_prepare(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st) {
     return GT_OK;
 }
 
+// Threads per linker block for frames of H x W pixels, its resident blocks
+// per SM (queried once per context) and its shared-memory pool.
+int link_shape(gt_ctx* ctx, long long px, int* nt, int* per_sm, int* pool) {
+    const bool big = px >= LINK_BIG_PIXELS;
+    *nt = big ? 1024 : 256;
+    *pool = big ? LINK_POOL_BYTES_BIG : LINK_POOL_BYTES;
+    int& cached = big ? ctx->link_per_sm_big : ctx->link_per_sm;
+    if (!cached) {
+        int q = 0;
+        CK(link_fixpoint_occupancy(*nt, *pool, &q));
+        cached = std::max(1, q);
+    }
+    *per_sm = cached;
+    return GT_OK;
+}
+
 int link_window(gt_ctx* ctx, const Plan& P, const Work& w, cudaStream_t st, int tb, int te, int wi) {
     LinkBufs L = link_bufs(P, w, ctx->subnet_budget);
     L.tb = tb;
     L.te = te;
     const int T = P.T;
     int rounds = 0;
-    L.lsm_bytes = LINK_POOL_BYTES;
-    if (!ctx->link_per_sm) {
-        CK(cudaFuncSetAttribute(link_fixpoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.lsm_bytes));
-        int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, link_fixpoint_kernel, 256, L.lsm_bytes));
-        ctx->link_per_sm = std::max(1, per_sm);
-    }
-    const int grid = std::max(1, std::min(P.nslot, ctx->link_per_sm * ctx->num_sms));
+    int nt = 256, per_sm = 1, pool = LINK_POOL_BYTES;
+    int rc = link_shape(ctx, (long long)P.H * P.W, &nt, &per_sm, &pool);
+    if (rc) return rc;
+    L.lsm_bytes = pool;
+    const int grid = std::max(1, std::min(P.nslot, per_sm * ctx->num_sms));
     int memory = (int)P.r.memory;
     int max_passes = te - tb + 1;
     int* ndirty = w.ndirty + (size_t)wi * (T + 2);
     int* passes = w.err + 1;
     unsigned long long* phase_ns = w.phase_ns;
     void* args[] = {&L, &memory, &max_passes, &rounds, &ndirty, &passes, &phase_ns};
-    CK(cudaLaunchCooperativeKernel((const void*)link_fixpoint_kernel, dim3(grid), dim3(256), args, L.lsm_bytes,
-                                   st));
+    CK(launch_link_fixpoint(nt, grid, args, pool, st));
     ctx->stats.launches += 1;
     return GT_OK;
 }
@@ -1155,8 +1173,7 @@ int enqueue_batch(gt_ctx* ctx, std::vector<BatchMovie>& B, gt_movie* mv, int n, 
         int* ps = bm.w.err + 1;
         unsigned long long* ph = bm.w.phase_ns;
         void* args[] = {&L, &memory, &max_passes, &rounds, &nd, &ps, &ph};
-        CK(cudaLaunchCooperativeKernel((const void*)link_fixpoint_kernel, dim3(bm.solo_grid), dim3(256), args,
-                                       LINK_POOL_BYTES, st));
+        CK(launch_link_fixpoint(256, bm.solo_grid, args, LINK_POOL_BYTES, st));
         S.launches += 1;
     }
     CK(cudaEventRecord(ctx->bev[9], st));
@@ -1236,8 +1253,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
     int per_sm_multi = 0, per_sm_solo = 0;
     CK(cudaFuncSetAttribute(link_fixpoint_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, LINK_POOL_BYTES));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_multi, link_fixpoint_multi_kernel, 256, LINK_POOL_BYTES));
-    CK(cudaFuncSetAttribute(link_fixpoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, LINK_POOL_BYTES));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_solo, link_fixpoint_kernel, 256, LINK_POOL_BYTES));
+    CK(link_fixpoint_occupancy(256, LINK_POOL_BYTES, &per_sm_solo));
     const size_t full_grid = (size_t)std::max(1, per_sm_multi) * ctx->num_sms;
     long long st_s = 1, st_s1 = 1, st_p1 = 1, st_n = 1, st_e = 1, st_h = 64;        // shared launch
     long long bt_s = 1, bt_s1 = 1, bt_p1 = 1, bt_n = 1, bt_e = 1, bt_h = 64;        // solo launches

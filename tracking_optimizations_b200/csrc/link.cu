@@ -26,7 +26,8 @@ namespace gt {
 
 
 namespace {
-constexpr int NTL = 256;
+constexpr int NTL = 256;   // threads of a linker block for small frames
+constexpr int NTL_BIG = 1024;  // for large frames: one block per SM, 32 warps per frame
 
 __device__ __forceinline__ bool within_r(float qy, float qx, float iy, float ix, float r, float* dist) {
     // kd-tree box pre-filter + linking.rs:91-100 distance (dest - source)
@@ -67,12 +68,13 @@ __device__ void uf_union(int* uf, int a, int b) {
     }
 }
 
+template <int NT>
 __device__ int block_scan_inplace_l(int* data, int n, int* warp_tot, int* s_total) {
-    const int chunk = (n + NTL - 1) / NTL;
+    const int chunk = (n + NT - 1) / NT;
     const int q0 = threadIdx.x * chunk, q1 = min(q0 + chunk, n);
     int mine = 0;
     for (int q = q0; q < q1; ++q) mine += data[q];
-    int pos = block_excl_scan<NTL>(mine, warp_tot, s_total);
+    int pos = block_excl_scan<NT>(mine, warp_tot, s_total);
     for (int q = q0; q < q1; ++q) { int v = data[q]; data[q] = pos; pos += v; }
     __syncthreads();
     return *s_total;
@@ -145,8 +147,9 @@ __device__ bool solve_subnet(const LinkBufs& L, const int* dests, int nd, const 
 }  // namespace
 
 // One CTA per frame (grid-stride); frame t >= 1 links P(t-1) + M(t) to P(t).
+template <int NT>
 __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int tstride) {
-    __shared__ int warp_tot[NTL / 32];
+    __shared__ int warp_tot[NT / 32];
     __shared__ int s_total;
     __shared__ int s_bump;
     extern __shared__ __align__(16) int lsm[];  // per-frame scratch pool
@@ -162,7 +165,7 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
         const int nd = L.npart[t];
         int* pred = L.pred + L.off[t];
         if (t == 0) {
-            for (int i = threadIdx.x; i < nd; i += NTL) pred[i] = -1;
+            for (int i = threadIdx.x; i < nd; i += NT) pred[i] = -1;
             __syncthreads();
         } else {
             const int n1 = L.npart[t - 1];
@@ -193,10 +196,10 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
                 const float* px_t = L.px + (size_t)t * cap_p;
                 const int* gs_t = L.gstart + (size_t)t * (ncell + 1);
                 const int* gi_t = L.gidx + (size_t)t * cap_p;
-                for (int i = threadIdx.x; i < nd; i += NTL) { ddy[i] = py_t[i]; ddx[i] = px_t[i]; ggi[i] = gi_t[i]; }
+                for (int i = threadIdx.x; i < nd; i += NT) { ddy[i] = py_t[i]; ddx[i] = px_t[i]; ggi[i] = gi_t[i]; }
                 if (grid_sm) {
                     int* ggs = take(ncell + 1);
-                    for (int i = threadIdx.x; i <= ncell; i += NTL) ggs[i] = gs_t[i];
+                    for (int i = threadIdx.x; i <= ncell; i += NT) ggs[i] = gs_t[i];
                     gs = ggs;
                 } else {
                     gs = gs_t;
@@ -227,7 +230,7 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
             int* bump = &s_bump;
             if (threadIdx.x == 0) *bump = 0;
             // sources: P(t-1) then M(t) (linking.rs:244-259 order)
-            for (int s = threadIdx.x; s < ns; s += NTL) {
+            for (int s = threadIdx.x; s < ns; s += NT) {
                 int h;
                 if (s < n1) h = (t - 1) * cap_p + s;
                 else h = __ldcg(L.mlist + (size_t)t * L.cap_m + (s - n1));
@@ -235,10 +238,10 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
                 sy[s] = L.py[h];
                 sx[s] = L.px[h];
             }
-            for (int s = threadIdx.x; s < n1; s += NTL) L.lnext[(size_t)(t - 1) * cap_p + s] = 0;
+            for (int s = threadIdx.x; s < n1; s += NT) L.lnext[(size_t)(t - 1) * cap_p + s] = 0;
             __syncthreads();
             // candidate pairs: degree pass
-            for (int s = threadIdx.x; s < ns; s += NTL) {
+            for (int s = threadIdx.x; s < ns; s += NT) {
                 const float qy = sy[s], qx = sx[s];
                 const int c = cell_of(qy, qx, G, L.ncy, L.ncx);
                 const int cy0 = c / L.ncx, cx0 = c - cy0 * L.ncx;
@@ -260,7 +263,7 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
                 sdeg[s] = deg;
             }
             __syncthreads();
-            const int ne = block_scan_inplace_l(sdeg, ns, warp_tot, &s_total);
+            const int ne = block_scan_inplace_l<NT>(sdeg, ns, warp_tot, &s_total);
             if (threadIdx.x == 0) sdeg[ns] = ne;
             int *edst, *dsrc;
             float *ew, *dw;
@@ -274,14 +277,14 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
             }
             if (ne > L.cap_e) {
                 if (threadIdx.x == 0) atomicOr(L.err, ERR_EDGE_OVERFLOW);
-                for (int i = threadIdx.x; i < nd; i += NTL) pred[i] = -1;
+                for (int i = threadIdx.x; i < nd; i += NT) pred[i] = -1;
                 __syncthreads();
                 continue;
             }
-            for (int i = threadIdx.x; i <= nd; i += NTL) dcnt[i] = 0;
+            for (int i = threadIdx.x; i <= nd; i += NT) dcnt[i] = 0;
             __syncthreads();
             // fill, then order each source's list by destination index
-            for (int s = threadIdx.x; s < ns; s += NTL) {
+            for (int s = threadIdx.x; s < ns; s += NT) {
                 const float qy = sy[s], qx = sx[s];
                 const int c = cell_of(qy, qx, G, L.ncy, L.ncx);
                 const int cy0 = c / L.ncx, cx0 = c - cy0 * L.ncx;
@@ -309,14 +312,14 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
             __syncthreads();
             // per-destination counts in a pass of their own: atomics inside
             // the neighbour search above stall it several-fold
-            for (int q = threadIdx.x; q < ne; q += NTL) atomicAdd(&dcnt[edst[q]], 1);
+            for (int q = threadIdx.x; q < ne; q += NT) atomicAdd(&dcnt[edst[q]], 1);
             __syncthreads();
-            block_scan_inplace_l(dcnt, nd + 1, warp_tot, &s_total);
+            block_scan_inplace_l<NT>(dcnt, nd + 1, warp_tot, &s_total);
             // destination lists, ascending source index (linking.rs:310-315)
             int* dcur = cmin;  // reuse: cursors per destination
-            for (int d = threadIdx.x; d < nd; d += NTL) dcur[d] = dcnt[d];
+            for (int d = threadIdx.x; d < nd; d += NT) dcur[d] = dcnt[d];
             __syncthreads();
-            for (int s = threadIdx.x; s < ns; s += NTL) {
+            for (int s = threadIdx.x; s < ns; s += NT) {
                 for (int q = sdeg[s]; q < sdeg[s + 1]; ++q) {
                     const int d = edst[q];
                     const int k = atomicAdd(&dcur[d], 1);
@@ -325,7 +328,7 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
                 }
             }
             __syncthreads();
-            for (int d = threadIdx.x; d < nd; d += NTL) {
+            for (int d = threadIdx.x; d < nd; d += NT) {
                 const int a = dcnt[d], e = dcnt[d + 1];
                 for (int q = a + 1; q < e; ++q) {
                     const int ks = dsrc[q];
@@ -336,20 +339,20 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
                 }
             }
             // union-find over sources [0, ns) and destinations [ns, ns + nd)
-            for (int i = threadIdx.x; i < nnode; i += NTL) {
+            for (int i = threadIdx.x; i < nnode; i += NT) {
                 uf[i] = i; cnd[i] = 0; cns[i] = 0; vis[i] = 0;
             }
             __syncthreads();
-            for (int s = threadIdx.x; s < ns; s += NTL)
+            for (int s = threadIdx.x; s < ns; s += NT)
                 for (int q = sdeg[s]; q < sdeg[s + 1]; ++q) uf_union(uf, s, ns + edst[q]);
             __syncthreads();
-            for (int i = threadIdx.x; i < nnode; i += NTL) uf[i] = uf_find(uf, i);
+            for (int i = threadIdx.x; i < nnode; i += NT) uf[i] = uf_find(uf, i);
             __syncthreads();
-            for (int i = threadIdx.x; i < nnode; i += NTL) cmin[i] = 0x7fffffff;
+            for (int i = threadIdx.x; i < nnode; i += NT) cmin[i] = 0x7fffffff;
             __syncthreads();
-            for (int s = threadIdx.x; s < ns; s += NTL)
+            for (int s = threadIdx.x; s < ns; s += NT)
                 if (sdeg[s + 1] > sdeg[s]) atomicAdd(&cns[uf[s]], 1);
-            for (int d = threadIdx.x; d < nd; d += NTL) {
+            for (int d = threadIdx.x; d < nd; d += NT) {
                 const int rt = uf[ns + d];
                 atomicAdd(&cnd[rt], 1);
                 atomicMin(&cmin[rt], d);
@@ -357,7 +360,7 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
             __syncthreads();
             // components, each resolved by the thread of its first destination
             const float null_cost = r * r;
-            for (int d = threadIdx.x; d < nd; d += NTL) {
+            for (int d = threadIdx.x; d < nd; d += NT) {
                 const int rt = uf[ns + d];
                 if (cmin[rt] != d) continue;
                 const int cd = cnd[rt], cs = cns[rt];
@@ -421,11 +424,11 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
         }
         // rank of each new particle within the frame (linking.rs:470)
         int* nr = L.newrank + L.off[t];
-        const int chunk = (nd + NTL - 1) / NTL;
+        const int chunk = (nd + NT - 1) / NT;
         const int q0 = threadIdx.x * chunk, q1 = min(q0 + chunk, nd);
         int mine = 0;
         for (int q = q0; q < q1; ++q) mine += (pred[q] < 0);
-        int pos = block_excl_scan<NTL>(mine, warp_tot, &s_total);
+        int pos = block_excl_scan<NT>(mine, warp_tot, &s_total);
         for (int q = q0; q < q1; ++q) nr[q] = pred[q] < 0 ? pos++ : -1;
         if (threadIdx.x == 0) L.newcount[t] = s_total;
         __syncthreads();
@@ -437,8 +440,9 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
 // linking.rs:479-485, oldest list first, index order within a list),
 // skipping trajectories present in frame t-1 and keeping the first entry of
 // each trajectory.  Marks frames whose M changed.
+template <int NT>
 __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, int tstride) {
-    __shared__ int warp_tot[NTL / 32];
+    __shared__ int warp_tot[NT / 32];
     __shared__ int s_total;
     __shared__ int s_diff;
     __shared__ int s_red;
@@ -458,7 +462,7 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
             for (int f = fbeg; f <= fend; ++f) {
                 const int n = L.npart[f];
                 const unsigned char* ln = L.lnext + (size_t)f * cap_p;
-                for (int i = threadIdx.x; i < n; i += NTL) cnt += __ldcg(ln + i) ? 0 : 1;
+                for (int i = threadIdx.x; i < n; i += NT) cnt += __ldcg(ln + i) ? 0 : 1;
             }
             atomicAdd(&s_red, cnt);
         }
@@ -491,10 +495,10 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
         for (int f = fbeg; f <= fend; ++f) {
             const int n = L.npart[f];
             const unsigned char* ln = L.lnext + (size_t)f * cap_p;
-            for (int i = threadIdx.x; i < n; i += NTL) cpos[i] = __ldcg(ln + i) ? 0 : 1;
+            for (int i = threadIdx.x; i < n; i += NT) cpos[i] = __ldcg(ln + i) ? 0 : 1;
             __syncthreads();
-            const int k = block_scan_inplace_l(cpos, n, warp_tot, &s_total);
-            for (int i = threadIdx.x; i < n; i += NTL) {
+            const int k = block_scan_inplace_l<NT>(cpos, n, warp_tot, &s_total);
+            for (int i = threadIdx.x; i < n; i += NT) {
                 if (__ldcg(ln + i)) continue;
                 const int j = nc + cpos[i];
                 if (j < lim) {
@@ -510,10 +514,10 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
         int* k1 = hk;
         int* k2 = hk + hs1;
         int* v2 = hv + hs1;
-        for (int i = threadIdx.x; i < hs1 + hs2; i += NTL) { hk[i] = -1; hv[i] = 0x7fffffff; }
+        for (int i = threadIdx.x; i < hs1 + hs2; i += NT) { hk[i] = -1; hv[i] = 0x7fffffff; }
         __syncthreads();
         // trajectories present in frame t-1
-        for (int i = threadIdx.x; i < n1; i += NTL) {
+        for (int i = threadIdx.x; i < n1; i += NT) {
             const int key = __ldcg(L.root + L.off[t - 1] + i);
             unsigned hsh = ((unsigned)key * 2654435761u) & (hs1 - 1);
             while (true) {
@@ -523,7 +527,7 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
             }
         }
         // first candidate of each trajectory
-        for (int j = threadIdx.x; j < nc; j += NTL) {
+        for (int j = threadIdx.x; j < nc; j += NT) {
             const int key = cr[j];
             unsigned hsh = ((unsigned)key * 2654435761u) & (hs2 - 1);
             while (true) {
@@ -534,7 +538,7 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
             atomicMin(&v2[hsh], j);
         }
         __syncthreads();
-        for (int j = threadIdx.x; j < nc; j += NTL) {
+        for (int j = threadIdx.x; j < nc; j += NT) {
             const int key = cr[j];
             bool keep = true;
             unsigned hsh = ((unsigned)key * 2654435761u) & (hs1 - 1);
@@ -553,20 +557,20 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
         }
         if (threadIdx.x == 0) s_diff = 0;
         __syncthreads();
-        const int nk = block_scan_inplace_l(cpos, nc, warp_tot, &s_total);
+        const int nk = block_scan_inplace_l<NT>(cpos, nc, warp_tot, &s_total);
         int* ml = L.mlist + (size_t)t * L.cap_m;
         const int old = __ldcg(L.mcount + t);
         if (nk > L.cap_m) { if (threadIdx.x == 0) atomicOr(L.err, ERR_MEM_OVERFLOW); continue; }
         if (old != nk && threadIdx.x == 0) s_diff = 1;
         __syncthreads();
-        for (int j = threadIdx.x; j < nc; j += NTL) {
+        for (int j = threadIdx.x; j < nc; j += NT) {
             const int a = cpos[j];
             const int nxt = (j + 1 < nc) ? cpos[j + 1] : nk;
             if (nxt > a && __ldcg(ml + a) != ch[j]) s_diff = 1;
         }
         __syncthreads();
         if (s_diff) {
-            for (int j = threadIdx.x; j < nc; j += NTL) {
+            for (int j = threadIdx.x; j < nc; j += NT) {
                 const int a = cpos[j];
                 const int nxt = (j + 1 < nc) ? cpos[j + 1] : nk;
                 if (nxt > a) ml[a] = ch[j];
@@ -660,13 +664,14 @@ __device__ __forceinline__ unsigned long long gtimer() {
 
 // phase_ns: [0] first linking, [1] roots, [2] memory entries, [3] relinking
 // (nanoseconds summed over passes, stamped by block 0 after each barrier)
-__global__ void __launch_bounds__(NTL, 4) link_fixpoint_kernel(LinkBufs L, int memory, int max_passes, int rounds,
+template <int NT>
+__global__ void __launch_bounds__(NT, NT == NTL ? 4 : 1) link_fixpoint_kernel(LinkBufs L, int memory, int max_passes, int rounds,
                                                                int* ndirty, int* passes,
                                                                unsigned long long* phase_ns) {
     cg::grid_group grid = cg::this_grid();
     const bool stamp = blockIdx.x == 0 && threadIdx.x == 0;
     unsigned long long t0 = stamp ? gtimer() : 0, acc[4] = {0, 0, 0, 0};
-    link_frames_body(L, 0, blockIdx.x, gridDim.x);
+    link_frames_body<NT>(L, 0, blockIdx.x, gridDim.x);
     int k = 0;
     if (memory > 0 && L.te > 2) {
         for (k = 1; k <= max_passes; ++k) {
@@ -675,11 +680,11 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_kernel(LinkBufs L, int m
             roots_body(L, grid);
             grid.sync();
             if (stamp) { const unsigned long long t = gtimer(); acc[1] += t - t0; t0 = t; }
-            memory_body(L, memory, ndirty + k, blockIdx.x, gridDim.x);
+            memory_body<NT>(L, memory, ndirty + k, blockIdx.x, gridDim.x);
             grid.sync();
             if (stamp) { const unsigned long long t = gtimer(); acc[2] += t - t0; t0 = t; }
             if (*(volatile int*)(ndirty + k) == 0) break;
-            link_frames_body(L, 1, blockIdx.x, gridDim.x);
+            link_frames_body<NT>(L, 1, blockIdx.x, gridDim.x);
         }
     }
     grid.sync();
@@ -692,6 +697,25 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_kernel(LinkBufs L, int m
         for (int i = 0; i < 4; ++i) phase_ns[i] += acc[i];
     }
     (void)rounds;
+}
+
+template __global__ void link_fixpoint_kernel<NTL>(LinkBufs, int, int, int, int*, int*, unsigned long long*);
+template __global__ void link_fixpoint_kernel<NTL_BIG>(LinkBufs, int, int, int, int*, int*, unsigned long long*);
+
+// Host side: the kernel for `nt` threads per block (256 or 1024), its
+// resident blocks per SM, and a cooperative launch of it.
+static const void* link_fixpoint_fn(int nt) {
+    return nt == NTL_BIG ? (const void*)link_fixpoint_kernel<NTL_BIG> : (const void*)link_fixpoint_kernel<NTL>;
+}
+
+cudaError_t link_fixpoint_occupancy(int nt, int smem, int* per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(link_fixpoint_fn(nt), cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, link_fixpoint_fn(nt), nt, smem);
+}
+
+cudaError_t launch_link_fixpoint(int nt, int grid, void** args, int smem, cudaStream_t st) {
+    return cudaLaunchCooperativeKernel(link_fixpoint_fn(nt), dim3(grid), dim3(nt), args, smem, st);
 }
 
 // Several movies in one cooperative launch (the batched path): every phase
@@ -709,7 +733,7 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_multi_kernel(const LinkB
     auto t0_of = [&](int m) { const int s = fstart[m] % G; return ((int)blockIdx.x - s + G) % G; };
     bool any_mem = false;
     for (int m = 0; m < nm; ++m) {
-        link_frames_body(Ls[m], 0, t0_of(m), G);
+        link_frames_body<NTL>(Ls[m], 0, t0_of(m), G);
         any_mem |= memory[m] > 0 && Ls[m].T > 2;
     }
     // ndirty[k * nm + m]: frames of movie m changed by pass k.  A movie
@@ -729,13 +753,13 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_multi_kernel(const LinkB
                 if (active(m, k)) roots_global(Ls[m]);
             grid.sync();
             for (int m = 0; m < nm; ++m)
-                if (active(m, k)) memory_body(Ls[m], memory[m], ndirty + k * nm + m, t0_of(m), G);
+                if (active(m, k)) memory_body<NTL>(Ls[m], memory[m], ndirty + k * nm + m, t0_of(m), G);
             grid.sync();
             int total = 0;
             for (int m = 0; m < nm; ++m) total += *(volatile int*)(ndirty + k * nm + m);
             if (total == 0) break;
             for (int m = 0; m < nm; ++m)
-                if (*(volatile int*)(ndirty + k * nm + m) > 0) link_frames_body(Ls[m], 1, t0_of(m), G);
+                if (*(volatile int*)(ndirty + k * nm + m) > 0) link_frames_body<NTL>(Ls[m], 1, t0_of(m), G);
         }
     }
     grid.sync();
