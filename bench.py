@@ -405,6 +405,40 @@ def run_batched(args, rank, world, local):
         batch_ms = timed(batch_step, args.steps)
     frames = sum(s.frames for s in specs)
     px = sum(s.frames * s.height * s.width for s in specs)
+    # the same comparison per class of frame size: which movies bound the ratio
+    classes = {"small (<= 256x512)": lambda s: s.height * s.width <= 256 * 512,
+               "medium (<= 1024x1024)": lambda s: 256 * 512 < s.height * s.width <= 1024 * 1024,
+               "large (> 1024x1024)": lambda s: s.height * s.width > 1024 * 1024}
+    per_class = {}
+    for name, pred in classes.items():
+        idx = [i for i, s in enumerate(specs) if pred(s)]
+        if not idx:
+            continue
+        sub = (_native.GtMovie * len(idx))()
+        for j, i in enumerate(idx):
+            sub[j] = arr[i]
+
+        def plain_c():
+            for i in idx:
+                fr, _ = movies[i]
+                T, H, W = fr.shape
+                _native.check(lib.gt_batch_device(ctx, ctypes.c_void_p(fr.data_ptr()), _native.GT_U16, T, H, W,
+                                                  ctypes.byref(plain_params[i]),
+                                                  ctypes.c_void_p(outs[i].data_ptr()), outs[i].shape[0],
+                                                  ctypes.byref(nrows), sp), ctx)
+
+        def batch_c():
+            _native.check(lib.gt_batch_many_device(ctx, sub, len(idx), sp), ctx)
+
+        for _ in range(2):
+            plain_c()
+            batch_c()
+        pm, bm = timed(plain_c, max(1, args.steps // 2)), timed(batch_c, max(1, args.steps // 2))
+        cf = sum(specs[i].frames for i in idx)
+        per_class[name] = {"movies": len(idx), "frames": cf,
+                           "gpx": sum(specs[i].frames * specs[i].height * specs[i].width for i in idx) / 1e9,
+                           "plain_ms": pm, "batched_ms": bm, "batched_over_plain": pm / bm,
+                           "plain_frames_per_s": cf / (pm / 1e3), "batched_frames_per_s": cf / (bm / 1e3)}
     if rank != 0:
         return
     peak, kind = peaks()
@@ -421,6 +455,7 @@ def run_batched(args, rank, world, local):
         "plain": {"value": frames / (plain_ms / 1e3), "ms_per_step": plain_ms,
                   "calls_per_step": len(specs)},
         "batched_over_plain": plain_ms / batch_ms,
+        "per_class": per_class,
         "roofline": {"bound": "hbm", "kernel": "whole batched step", "achieved": alg / (batch_ms / 1e3) / 1e9,
                      "peak": peak, "peak_kind": kind, "unit": "GB/s",
                      "frac": alg / (batch_ms / 1e3) / 1e9 / peak, "traffic": None, "algorithmic_bytes": alg},

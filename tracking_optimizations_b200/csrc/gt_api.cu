@@ -998,6 +998,8 @@ struct BatchMovie {
     bool solo = false;   // linked by its own cooperative launch (large movie)
     LinkBufs solo_L{};
     int solo_grid = 0;
+    int solo_nt = 256;   // threads per block of its own linker launch
+    int solo_pool = 0;   // and that launch's shared-memory pool
 };
 
 struct BatchShared {
@@ -1173,7 +1175,7 @@ int enqueue_batch(gt_ctx* ctx, std::vector<BatchMovie>& B, gt_movie* mv, int n, 
         int* ps = bm.w.err + 1;
         unsigned long long* ph = bm.w.phase_ns;
         void* args[] = {&L, &memory, &max_passes, &rounds, &nd, &ps, &ph};
-        CK(launch_link_fixpoint(256, bm.solo_grid, args, LINK_POOL_BYTES, st));
+        CK(launch_link_fixpoint(bm.solo_nt, bm.solo_grid, args, bm.solo_pool, st));
         S.launches += 1;
     }
     CK(cudaEventRecord(ctx->bev[9], st));
@@ -1318,8 +1320,11 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         const Plan& P = B[i].P;
         const size_t own = slot_bytes(P.cap_s, (long long)P.cap_s + 1, (long long)P.cap_p + 1,
                                       (long long)P.cap_s + P.cap_p, P.cap_e, P.hsize);
+        int per_sm_own = 1;
+        int rc_s = link_shape(ctx, (long long)P.H * P.W, &B[i].solo_nt, &per_sm_own, &B[i].solo_pool);
+        if (rc_s) return rc_s;
         B[i].solo_grid = (int)std::max<size_t>(1, std::min<size_t>({(size_t)P.T,
-                                                                   (size_t)std::max(1, per_sm_solo) * ctx->num_sms,
+                                                                   (size_t)per_sm_own * ctx->num_sms,
                                                                    budget / own}));
         Carver dry{nullptr};
         Work wd{};
@@ -1419,7 +1424,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         L.d_w = pool_big.d_w; L.uf = pool_big.uf; L.c_nd = pool_big.c_nd; L.c_ns = pool_big.c_ns;
         L.c_min = pool_big.c_min; L.vis = pool_big.vis; L.work = pool_big.work; L.bump = pool_big.bump;
         L.hkey = pool_big.hkey; L.hval = pool_big.hval;
-        L.lsm_bytes = LINK_POOL_BYTES;  // slot strides: the movie's own (link_bufs)
+        L.lsm_bytes = B[i].solo_pool;  // slot strides: the movie's own (link_bufs)
         B[i].solo_L = L;
     }
     if (!replay) {

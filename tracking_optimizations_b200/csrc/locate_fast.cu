@@ -21,11 +21,11 @@
 //      scales by the reciprocal of the Gaussian norm, subtracts the boxcar
 //      as fma(-box, 1/k^2, gauss) and clips at 0 -> P2 (row pairs);
 //   3. row max over the dilation window (register sliding max) -> RM2;
-//   4. column max of RM2 compared with the centre -> local-max flags;
-//   5. the flagged pixels are listed by ballots and walked one per lane by
-//      as few warps as they need; those warps compute the features and
-//      emit the records (ranks from per-row bit masks, one slot atomic per
-//      warp).
+//   4. column max of RM2 compared with the centre: the local maxima of a
+//      warp's rows are listed at once by per-row ballots into the CTA list;
+//   5. the list is walked one candidate per lane by as few warps as it
+//      needs; those warps compute the features and emit the records (ranks
+//      from per-row bit masks, one slot atomic per warp).
 // Row strides of the pair arrays are odd (in 8-byte units), so every
 // lane-per-row access is bank-conflict free.
 #include <cuda.h>
@@ -108,7 +108,8 @@ struct Geo {
     static_assert((NPW - 1) * FM < US && (FM * 2) % 16 == 0, "16-byte raw loads start inside a U row");
     static_assert(SMEM <= 227 * 1024, "shared memory");
     static_assert(RC + 2 <= HP && RC <= HX, "walk and feature circles inside the processed region");
-    static_assert(TH0 * FT + (fast_threads(TH0) / 32) * 32 * 20 <= SZ_BP, "emission staging fits the dead boxcar region");
+    static_assert(TH0 * FT * 4 + (fast_threads(TH0) / 32) * 32 * 20 <= SZ_BP,
+                  "candidate list and emission staging fit the dead boxcar region");
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -335,8 +336,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     float2* Bp = (float2*)(smem + G::OFF_BP);
     unsigned short* U = (unsigned short*)(smem + G::OFF_U);  // raw tile, row stride US
     float2* RM2 = Gp;                           // after the column pass
-    int* clist = (int*)Gp;                      // after the local-max pass
-    unsigned char* flags = (unsigned char*)Bp;  // after the column pass
+    int* clist = (int*)Bp;                      // candidate list: the boxcar is dead after the column pass
     float2* sc = (float2*)(smem + G::OFF_TAB);  // (sin2, cos2) of the d/2 circle
 
     // ---- 0. stage the raw tile ----
@@ -474,23 +474,26 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         if (fr0 >= 0 && fr0 + FM + 2 * KR - 1 < H) {
 #pragma unroll
             for (int k = 0; k < FM / 2 + KR; ++k) L[k] = Bp[(p0 + k) * G::GPS + c];
+            // the rows' box sums in scalar: the first window summed in tap
+            // order, each next row's window slid by one row; every partial
+            // sum is an integer below 2^24 (u16 frames), so all orders give
+            // the same bits
+            float b[FM + 2 * KR];
 #pragma unroll
-            for (int k = 0; k < FM / 2 + KR - 1; ++k) ML[k] = make_float2(L[k].y, L[k + 1].x);
-            // the first window summed in tap order, the next ones slid by
-            // one row pair; every partial sum is an integer below 2^24
-            // (u16 frames), so all orders give the same bits
-            {
-                float2 s = L[0];
+            for (int k = 0; k < FM / 2 + KR; ++k) { b[2 * k] = L[k].x; b[2 * k + 1] = L[k].y; }
+            float sb[FM];
+            float s0 = b[0];
 #pragma unroll
-                for (int j = 1; j < TAPS; ++j) s = add2(s, (j & 1) ? ML[j >> 1] : L[j >> 1]);
-                cs[0] = s;
+            for (int j = 1; j < TAPS; ++j) s0 = s0 + b[j];
+            sb[0] = s0;
 #pragma unroll
-                for (int m = 0; m + 1 < FM / 2; ++m) {
-                    s = add2(add2(s, L[m + 1 + KR]), ML[m + KR]);
-                    s = sub2(sub2(s, L[m]), ML[m]);
-                    cs[m + 1] = s;
-                }
+            for (int m = 1; m < FM; ++m) {
+                s0 = s0 + b[m + 2 * KR];
+                s0 = s0 - b[m - 1];
+                sb[m] = s0;
             }
+#pragma unroll
+            for (int m = 0; m < FM / 2; ++m) cs[m] = make_float2(sb[2 * m], sb[2 * m + 1]);
         } else {
             // reflect-padded boxcar at the top/bottom frame edges
             const float* Bf = (const float*)Bp;
@@ -517,9 +520,12 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             // preprocess_cols.wgsl:54 contracted: fma(-cs, 1/k^2, gauss);
             // cs * -rkk is exactly -(cs * rkk)
             const float2 res = fma2(cs[m], NRKK2, gq[m]);
+            // preprocess_cols.wgsl:55-60 clip at 0; res is never NaN or -0
+            // here (u16 frames, non-negative sums), where max equals the
+            // shader's select
             float2 o;
-            o.x = res.x < 0.f ? 0.f : res.x;  // preprocess_cols.wgsl:55-60
-            o.y = res.y < 0.f ? 0.f : res.y;
+            o.x = fmaxf(res.x, 0.f);
+            o.y = fmaxf(res.y, 0.f);
             if (!all_in) {
                 const int fa = fa0 + 2 * m;
                 if (!(cin && fa >= 0 && fa < H)) o.x = NEG;
@@ -550,9 +556,17 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     }
     __syncthreads();
 
-    // ---- 4. column max vs centre: non-strict local max (walk_cols.wgsl:19-36) ----
-    for (int it = tid; it < FT * (TH0 / FM); it += NTK) {
-        const int tc = it % FT, rq = it / FT;
+    // ---- 4. column max vs centre: non-strict local max (walk_cols.wgsl:19-36),
+    //         listed at once: warp w owns tile rows 8 (w / 2) .. + 7 of
+    //         column half w % 2, ballots each row and appends its flagged
+    //         pixels to the CTA list (one shared atomic per warp; the order
+    //         of the list does not matter: records carry their rank) ----
+    constexpr int NW = NTK / 32;
+    static_assert(FT * (TH0 / FM) == NTK && FT == 64, "one column of 8 rows per thread");
+    const int warp = tid >> 5, lane = tid & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    {
+        const int tc = tid % FT, rq = tid / FT;
         const int tr0 = rq * FM;
         const int k0 = (tr0 + HP - O) >> 1;  // HP - O is even
         constexpr int NPR = (FM + DD - 1 + 1) / 2;
@@ -570,52 +584,37 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         slide_max<DD, FM>(v, cm);
         const float* Pf = (const float*)P2;
         const bool col_in = tx0 + tc < W;
+        unsigned bal[FM];
+        int nc = 0;
 #pragma unroll
         for (int m = 0; m < FM; ++m) {
             const int r = tr0 + m + HP;  // processed row of the centre
             const float center = Pf[(((r >> 1) * G::P2S + tc + HX) << 1) + (r & 1)];
             const bool in = col_in && tr0 + m < TH;
             const bool f = in && cm[m] <= center && !(p.zero_skip && center == 0.f);
-            flags[(tr0 + m) * FT + tc] = f ? 1 : 0;
-        }
-    }
-    __syncthreads();
-
-    // ---- 5. candidate list, walks packed 32 per warp, emission ----
-    // Each warp appends the flagged pixels of its own tile rows to the CTA
-    // list; the list is then walked one candidate per lane by as few warps
-    // as it needs (the other warps leave), so the walks, which are the
-    // costliest code per candidate, run with full warps.  Records are ranked
-    // within their (row, tile) segment from a per-row bit mask of the
-    // columns that emit, which is what finalize_kernel needs; slots come
-    // from one atomic per warp.  Candidates beyond one per thread of the
-    // CTA are emitted as pending without a walk; fallback_walk_kernel walks
-    // them.
-    constexpr int NW = NTK / 32;
-    constexpr int RPW = TH0 / NW;
-    static_assert(RPW * NW == TH0 && FT == 64, "warp row ownership");
-    const int warp = tid >> 5, lane = tid & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    {
-        unsigned bals[2 * RPW];
-        int nc = 0;
-#pragma unroll
-        for (int k = 0; k < 2 * RPW; ++k) {
-            const int q = (warp * RPW + (k >> 1)) * FT + (k & 1) * 32 + lane;
-            bals[k] = __ballot_sync(0xffffffffu, flags[q] != 0);
-            nc += __popc(bals[k]);
+            bal[m] = __ballot_sync(0xffffffffu, f);
+            nc += __popc(bal[m]);
         }
         int wbase = 0;
         if (lane == 0 && nc) wbase = atomicAdd(&s_nc, nc);
         wbase = __shfl_sync(0xffffffffu, wbase, 0);
 #pragma unroll
-        for (int k = 0; k < 2 * RPW; ++k) {
-            if ((bals[k] >> lane) & 1u)
-                clist[wbase + __popc(bals[k] & lt)] = (warp * RPW + (k >> 1)) * FT + (k & 1) * 32 + lane;
-            wbase += __popc(bals[k]);
+        for (int m = 0; m < FM; ++m) {
+            if ((bal[m] >> lane) & 1u) clist[wbase + __popc(bal[m] & lt)] = (tr0 + m) * FT + tc;
+            wbase += __popc(bal[m]);
         }
     }
     __syncthreads();
+
+    // ---- 5. walks and emission ----
+    // The list is walked one candidate per lane by as few warps as it needs
+    // (the other warps leave: the walks, the costliest code per candidate,
+    // run with full warps and cost the SM's other CTA few issue slots).
+    // Records are ranked within their (row, tile) segment from a per-row
+    // bit mask of the columns that emit, which is what finalize_kernel
+    // needs; slots come from one atomic per warp.  Candidates beyond one per
+    // thread of the CTA are emitted as pending without a walk;
+    // fallback_walk_kernel walks them.
     const int ncand = s_nc;
     const int nwalk = min(NW, max(1, (ncand + 31) >> 5));
     if (warp >= nwalk) return;  // only the named barrier below follows
@@ -669,14 +668,10 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         }
         nrec += __popc(__ballot_sync(0xffffffffu, more));
     }
+    // this warp's slots; the result is first needed at the stores, so the
+    // atomic's latency overlaps the barrier and the sums below
     int gbase = 0;
-    if (lane == 0 && nrec) {
-        gbase = atomicAdd(b.fcount + t, nrec);
-        if (gbase + nrec > b.cap_c) {
-            atomicOr(b.err, ERR_CAND_OVERFLOW);
-            gbase = -1;
-        }
-    }
+    if (lane == 0 && nrec) gbase = atomicAdd(b.fcount + t, nrec);
     if (nwalk > 1) asm volatile("bar.sync 1, %0;" ::"r"(wstride) : "memory");
     else __syncwarp();
     if (warp == 0)
@@ -691,8 +686,8 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     const unsigned short* frame = (const unsigned short*)b.frames + (size_t)t * H * W;
     GRawAcc racc{frame, W};
     const float* P2f = (const float*)P2;
-    int* stage = (int*)((unsigned char*)Bp + TH0 * FT) + warp * 32;  // flags are dead here
-    float4* sfeat = (float4*)((unsigned char*)Bp + TH0 * FT + NW * 32 * 4) + warp * 32;
+    int* stage = (int*)((unsigned char*)Bp + TH0 * FT * 4) + warp * 32;  // after the candidate list
+    float4* sfeat = (float4*)((unsigned char*)Bp + TH0 * FT * 4 + NW * 32 * 4) + warp * 32;
     int roff = 0;
     for (int c0 = 0; c0 < ncand; c0 += wstride) {
         int rq = q, rtr = tr, rtc = tc, rst = st;
@@ -731,7 +726,11 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         }
         // the slot base of lane 0's atomic, read only now: its latency
         // overlapped the sums above
-        const int gb = __shfl_sync(0xffffffffu, gbase, 0);
+        int gb = __shfl_sync(0xffffffffu, gbase, 0);
+        if (gb + nrec > b.cap_c) {
+            if (lane == 0 && c0 == 0) atomicOr(b.err, ERR_CAND_OVERFLOW);
+            gb = -1;
+        }
         if (em) {
             Cand rec;
             rec.u = ru; rec.v = rv;
