@@ -663,7 +663,11 @@ __device__ __forceinline__ unsigned long long gtimer() {
 }  // namespace
 
 // phase_ns: [0] first linking, [1] roots, [2] memory entries, [3] relinking
-// (nanoseconds summed over passes, stamped by block 0 after each barrier)
+// (nanoseconds summed over passes, stamped by block 0 after each barrier).
+// The memory entries of every frame are computed from one consistent state
+// (a grid barrier before and after): a frame read while another block
+// relinks its neighbour could see that neighbour's links half rewritten,
+// which inflates the entries and the subnetworks they form.
 template <int NT>
 __global__ void __launch_bounds__(NT, NT == NTL ? 4 : 1) link_fixpoint_kernel(LinkBufs L, int memory, int max_passes, int rounds,
                                                                int* ndirty, int* passes,
