@@ -587,6 +587,95 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
     }
 }
 
+// Memory entries M(t) for memory 1 or 2, without trajectory roots.
+//
+// With at most two memory lists no trajectory branches: a particle left
+// unused by the next frame is a memory candidate for the next two frames
+// only, and once it is linked as a memory entry its trajectory id is
+// present in the following frame, which excludes it there.  So, with ids
+// unique within a frame (every source links at most one destination):
+//   - a frame t-2 particle unused by frame t-1 never shares its id with a
+//     frame t-1 particle (memory links into t-1 come from frames t-4 and
+//     t-3) nor with a frame t-3 candidate (neither descends from the
+//     other, and a common ancestor would be a branch);
+//   - a frame t-3 particle unused by frame t-2 shares its id with a frame
+//     t-1 particle exactly when that particle's pred is it (it was linked
+//     into t-1 as a memory entry): it has no descendant in t-2.
+// linking.rs:244-259 (unused lists oldest first, index order within a
+// list, dedupe by id against prev and among the entries) thus gives:
+// M(t) = the frame t-3 particles unused by t-2 and not the pred of a
+// frame t-1 particle, then the frame t-2 particles unused by t-1 (memory 1:
+// the latter only).  Marks frames whose M changed.
+template <int NT>
+__device__ void memory_body_short(const LinkBufs& L, int memory, int* ndirty, int t0, int tstride) {
+    __shared__ int warp_tot[NT / 32];
+    __shared__ int s_total;
+    __shared__ int s_diff;
+    extern __shared__ __align__(16) int lsm[];
+    const int slot = blockIdx.x;
+    const int cap_p = L.cap_p;
+    const int pool = L.lsm_bytes / 4;
+    for (int t = L.tb + t0; t < L.te; t += tstride) {
+        const int fbeg = max(0, t - 1 - memory), fend = t - 2;
+        if (fend < fbeg) continue;
+        const int fo = (fend > fbeg) ? fbeg : -1;  // frame t-3 (memory 2)
+        const int no = fo >= 0 ? L.npart[fo] : 0;
+        const int nb = L.npart[fbeg], ne = L.npart[fend];
+        const int nmax = max(nb, ne);
+        const int ccap = nb + (fo >= 0 ? ne : 0);
+        int *taken, *cpos, *ch;
+        if (no + nmax + ccap + 1 <= pool) {
+            taken = lsm; cpos = taken + no; ch = cpos + nmax;
+        } else {
+            int* w = L.work + (size_t)slot * 4 * L.st_n;
+            taken = w; cpos = w + L.st_n; ch = w + 2 * L.st_n;
+        }
+        for (int i = threadIdx.x; i < no; i += NT) taken[i] = 0;
+        if (threadIdx.x == 0) s_diff = 0;
+        __syncthreads();
+        if (fo >= 0) {
+            const int o0 = L.off[fo], n1 = L.npart[t - 1];
+            const int* pr = L.pred + L.off[t - 1];
+            for (int x = threadIdx.x; x < n1; x += NT) {
+                const int p = __ldcg(pr + x);
+                if (p >= o0 && p < o0 + no) taken[p - o0] = 1;
+            }
+        }
+        __syncthreads();
+        int nc = 0;
+        for (int f = fbeg; f <= fend; ++f) {
+            const int n = L.npart[f];
+            const unsigned char* ln = L.lnext + (size_t)f * cap_p;
+            const bool old = f == fo;
+            for (int i = threadIdx.x; i < n; i += NT) cpos[i] = (__ldcg(ln + i) || (old && taken[i])) ? 0 : 1;
+            __syncthreads();
+            const int k = block_scan_inplace_l<NT>(cpos, n, warp_tot, &s_total);
+            for (int i = threadIdx.x; i < n; i += NT)
+                if (!(__ldcg(ln + i) || (old && taken[i]))) ch[nc + cpos[i]] = f * cap_p + i;
+            nc += k;
+            __syncthreads();
+        }
+        int* ml = L.mlist + (size_t)t * L.cap_m;
+        const int oldn = __ldcg(L.mcount + t);
+        if (nc > L.cap_m) { if (threadIdx.x == 0) atomicOr(L.err, ERR_MEM_OVERFLOW); continue; }
+        if (oldn != nc && threadIdx.x == 0) s_diff = 1;
+        for (int j = threadIdx.x; j < nc; j += NT)
+            if (__ldcg(ml + j) != ch[j]) s_diff = 1;
+        __syncthreads();
+        if (s_diff) {
+            for (int j = threadIdx.x; j < nc; j += NT) ml[j] = ch[j];
+            if (threadIdx.x == 0) {
+                L.mcount[t] = nc;
+                L.dirty[t] = 1;
+                atomicAdd(ndirty, 1);
+            }
+        } else if (threadIdx.x == 0) {
+            L.dirty[t] = 0;
+        }
+        __syncthreads();
+    }
+}
+
 // Trajectory roots (the first particle of each trajectory, compact index),
 // in two levels.  Compact indices run in frame order and a pred always
 // points to an earlier particle, so a chain only ever steps to smaller
@@ -678,13 +767,19 @@ __global__ void __launch_bounds__(NT, NT == NTL ? 4 : 1) link_fixpoint_kernel(Li
     link_frames_body<NT>(L, 0, blockIdx.x, gridDim.x);
     int k = 0;
     if (memory > 0 && L.te > 2) {
+        // memory 1 or 2: the entries need no trajectory roots
+        // (memory_body_short), so the roots are computed once, at the end
+        const bool short_mem = memory <= 2;
         for (k = 1; k <= max_passes; ++k) {
             grid.sync();
             if (stamp) { const unsigned long long t = gtimer(); acc[k == 1 ? 0 : 3] += t - t0; t0 = t; }
-            roots_body(L, grid);
-            grid.sync();
+            if (!short_mem) {
+                roots_body(L, grid);
+                grid.sync();
+            }
             if (stamp) { const unsigned long long t = gtimer(); acc[1] += t - t0; t0 = t; }
-            memory_body<NT>(L, memory, ndirty + k, blockIdx.x, gridDim.x);
+            if (short_mem) memory_body_short<NT>(L, memory, ndirty + k, blockIdx.x, gridDim.x);
+            else memory_body<NT>(L, memory, ndirty + k, blockIdx.x, gridDim.x);
             grid.sync();
             if (stamp) { const unsigned long long t = gtimer(); acc[2] += t - t0; t0 = t; }
             if (*(volatile int*)(ndirty + k) == 0) break;
@@ -751,13 +846,16 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_multi_kernel(const LinkB
         for (k = 1; k <= max_passes; ++k) {
             grid.sync();
             for (int m = 0; m < nm; ++m)
-                if (active(m, k)) roots_local(Ls[m]);
+                if (active(m, k) && memory[m] > 2) roots_local(Ls[m]);
             grid.sync();
             for (int m = 0; m < nm; ++m)
-                if (active(m, k)) roots_global(Ls[m]);
+                if (active(m, k) && memory[m] > 2) roots_global(Ls[m]);
             grid.sync();
-            for (int m = 0; m < nm; ++m)
-                if (active(m, k)) memory_body<NTL>(Ls[m], memory[m], ndirty + k * nm + m, t0_of(m), G);
+            for (int m = 0; m < nm; ++m) {
+                if (!active(m, k)) continue;
+                if (memory[m] <= 2) memory_body_short<NTL>(Ls[m], memory[m], ndirty + k * nm + m, t0_of(m), G);
+                else memory_body<NTL>(Ls[m], memory[m], ndirty + k * nm + m, t0_of(m), G);
+            }
             grid.sync();
             int total = 0;
             for (int m = 0; m < nm; ++m) total += *(volatile int*)(ndirty + k * nm + m);
