@@ -292,6 +292,10 @@ GT_API void gt_table_free(gt_table* table);
 /* Options of a context (no reference counterpart):
  *   "locate_tile_rows"  output tile height of the specialised locate kernel, 32 or 64
  *   "force_generic"     1 = always use the generic locate kernel
+ *   "locate_tiles_per_cta"
+ *                       output tiles located one after another by a CTA of
+ *                       the specialised kernel, 1-64 (0 = the default: up to
+ *                       8, as long as a launch keeps about four waves of CTAs)
  *   "autotune"          0 = gt_batch_many_device keeps the configured tile rows
  *   "normalized_taps"   1 = Gaussian taps divided by their sum on the host and
  *                       no division in the passes (kernels.rs:86-97 gauss_1d,

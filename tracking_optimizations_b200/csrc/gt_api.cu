@@ -100,6 +100,7 @@ struct gt_ctx {
     int withhold_tma = 0;             // test switch of the bounded tile-copy wait
     int force_generic = 0;            // always use locate_tiles_kernel
     int fast_tile_rows = 64;          // output tile height of the fast kernel (32 or 64)
+    int tiles_per_cta = 0;            // fast kernel: tiles per CTA (0 = chosen per launch)
     // batched path (gt_batch_many_device)
     std::map<std::array<int, 6>, int> tile_rows;  // autotuned tile rows per (H, W, krad, D, rc, dtype)
     std::string batch_key;            // inputs of the cached graph
@@ -933,6 +934,7 @@ int batch_common(gt_ctx* ctx, const void* frames, bool host, int dtype, int T, i
             P.lp.tma_withhold = 1;
             P.lp.tma_spin = 1 << 10;
         }
+        P.lp.tiles_per_cta = ctx->tiles_per_cta;
         const size_t fbytes = host ? (size_t)T * H * W * elem_size(dtype) : 0;
         Work w{};
         // a caller's device buffer receives the rows directly: no table slab
@@ -1221,6 +1223,7 @@ int batch_many(gt_ctx* ctx, gt_movie* mv, int n, cudaStream_t st) {
         rc = make_plan(r, m.T, m.H, m.W, m.dtype, 1, ctx->num_sms, &B[i].P, &msg, ctx->force_generic, ctx->fast_tile_rows,
                        ctx->batch_cap_div);
         if (rc) { ctx->err = who + msg; return rc; }
+        B[i].P.lp.tiles_per_cta = ctx->tiles_per_cta;
         char buf[128];
         std::snprintf(buf, sizeof(buf), "%p|%d|%d|%d|%d|%p|%lld|", m.frames, m.dtype, m.T, m.H, m.W, (void*)m.out,
                       (long long)m.out_rows);
@@ -1941,6 +1944,15 @@ int gt_ctx_set_option(gt_ctx* ctx, const char* key, int value) {
     if (k == "subnet_budget" && value > 0) { ctx->subnet_budget = value; return GT_OK; }
     if (k == "subnet_budget" && value == 0) { ctx->subnet_budget = SUBNET_BUDGET; return GT_OK; }
     if (k == "test_withhold_tile_copy" && (value == 0 || value == 1)) { ctx->withhold_tma = value; return GT_OK; }
+    if (k == "locate_tiles_per_cta" && value >= 0 && value <= 64) {
+        ctx->tiles_per_cta = value;
+        if (ctx->batch_exec) {  // the cached batch graph holds the old launch shape
+            cudaGraphExecDestroy(ctx->batch_exec);
+            ctx->batch_exec = nullptr;
+            ctx->batch_key.clear();
+        }
+        return GT_OK;
+    }
     if (k == "normalized_taps" && (value == 0 || value == 1)) {
         ctx->normalized_taps = value;
         if (ctx->batch_exec) {  // the cached batch graph holds the old taps

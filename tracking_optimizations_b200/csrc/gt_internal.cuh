@@ -42,6 +42,7 @@ struct LocParams {
     int n_gchar;                // entries of the (d-1)/2 circle table
     int tma_spin;               // iteration limit of the bounded wait for a staged tile
     int tma_withhold;           // test switch: issue no tile copy, so the wait runs out
+    int tiles_per_cta;          // specialised kernel: tiles per CTA (0 = chosen per launch)
 };
 
 // One located feature, keyed by its originating pixel (walk_cols.wgsl:87-91).

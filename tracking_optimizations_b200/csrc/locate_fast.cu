@@ -31,6 +31,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "gt_device.cuh"
@@ -46,6 +47,9 @@ constexpr int FNT = 256;  // threads of a 32-row tile
 // output row) keep 16 warps per SM slot at 2 CTAs per SM
 __host__ __device__ constexpr int fast_threads(int th) { return th == 32 ? FNT : 2 * FNT; }
 constexpr int FM = 8;     // outputs per thread item
+// walker warps of a run of tiles: at most this many walk a tile while the
+// other warps start the next one
+constexpr int NWO = 2;
 
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int round8(int x) { return (x + 7) / 8 * 8; }
@@ -56,6 +60,13 @@ __host__ __device__ constexpr int circle_size(int RC) {
     for (int i = -RC; i <= RC; ++i)
         for (int j = -RC; j <= RC; ++j) k += (i * i + j * j <= RC * RC);
     return k;
+}
+
+// CTAs of the specialised kernel per SM with `smem` bytes of dynamic shared
+// memory: 228 KB per SM, 1 KB reserved per CTA and about 1 KB of static
+// arrays; the registers allow 2 CTAs of 512 threads or 4 of 256.
+__host__ __device__ constexpr int fast_ctas(int th, int smem) {
+    return cmax(0, (th == 32 ? 4 : 2) < 233472 / (smem + 2048) ? (th == 32 ? 4 : 2) : 233472 / (smem + 2048));
 }
 
 // Compile-time tile geometry.
@@ -74,26 +85,35 @@ struct Geo {
     static constexpr int PW = RW - 2 * KR;
     static constexpr int NPW = (PW + FM - 1) / FM;
     static constexpr int PWC = FM * NPW;
-    static constexpr int NRQ = (PH + FM - 1) / FM;
+    static constexpr int NRQ = (PH + FM - 1) / FM;  // column-pass items per column
     static constexpr int GPS = PWC | 1;
-    static constexpr int P2S = PWC | 1;
+    static constexpr int P2S = PW | 1;
     static constexpr int RMS = FT | 1;
-    static constexpr int RPA = 4 * NRQ + KR;  // Gp/Bp row pairs allocated
     static constexpr int NV = (FM + 2 * KR + 7) / 8;  // 16-byte loads per raw row of a row-pass item
     // raw tile row stride: a row pair spans an odd number of 16-byte units
     // (quarter-warp 16-byte loads of consecutive row pairs hit 2 banks at most)
     static constexpr int US = ((RW / 8) % 2 == 0) ? RW + 8 : RW;
-    static constexpr int SZ_P2 = align128(4 * NRQ * P2S * 8);
+    static constexpr int NTK = fast_threads(TH0);
+    static constexpr int SZ_P2 = align128(PP * P2S * 8);
     static constexpr int SZ_U = align128(RH * US * 2 + 16 * NV);  // + the last item's overrun
-    static constexpr int SZ_GP = align128(cmax(cmax(RPA * GPS * 8, (PP + 1) * RMS * 8), TH0 * FT * 4));
-    static constexpr int SZ_BP = align128(cmax(RPA * GPS * 8, TH0 * FT));
+    static constexpr int SZ_GP = align128(cmax(RP * GPS * 8, (PP + 1) * RMS * 8));
+    // boxcar rows, then the candidate list (u16) and the walkers' emission staging
+    static constexpr int SZ_BP = align128(cmax(RP * GPS * 8, TH0 * FT * 2 + (NTK / 32) * 32 * 20));
     static constexpr int K = circle_size(RC);
     static constexpr int SZ_TAB = align128(K * 20);  // (sin2, cos2), P2 offsets by parity, r2
-    static constexpr int OFF_GP = SZ_P2;
+    static constexpr int SZ_STG = align128(NWO * 32 * 20);  // emission staging of the overlapping walkers
+    static constexpr int SMEM1 = SZ_P2 + SZ_GP + SZ_BP + SZ_U + SZ_TAB + SZ_STG;
+    // Two processed planes (the walkers read the previous tile's while the
+    // stencil warps write the next one) where that keeps the CTAs per SM.
+    static constexpr bool WS =
+        fast_ctas(TH0, SMEM1 + SZ_P2) >= fast_ctas(TH0, SMEM1) && SMEM1 + SZ_P2 <= 227 * 1024;
+    static constexpr int NP2 = WS ? 2 : 1;
+    static constexpr int OFF_GP = NP2 * SZ_P2;
     static constexpr int OFF_BP = OFF_GP + SZ_GP;
     static constexpr int OFF_U = OFF_BP + SZ_BP;
     static constexpr int OFF_TAB = OFF_U + SZ_U;
-    static constexpr int SMEM = OFF_TAB + SZ_TAB;
+    static constexpr int OFF_STG = OFF_TAB + SZ_TAB;
+    static constexpr int SMEM = OFF_STG + SZ_STG;
     // index invariants of the phases below
     static_assert(((HP - O) & 1) == 0, "row pairs of the local-max pass must align");
     static_assert(HX >= HP && HX - O >= 0, "row max window starts inside the processed region");
@@ -101,15 +121,15 @@ struct Geo {
     static_assert(((TH0 - FM + HP - O) >> 1) + (FM + DD) / 2 - 1 <= PP, "column max rows allocated");
     static_assert(TH0 - 1 + HP + (DD - 1 - O) <= PH - 1, "column max window inside the processed rows");
     static_assert(FT + HX <= PW, "centre columns computed");
-    static_assert(4 * (NRQ - 1) + FM / 2 + KR <= RPA, "column pass reads allocated row pairs");
-    static_assert((PH - 2) / 2 + KR <= RP - 1, "valid outputs read computed row pairs only");
-    static_assert(PWC <= GPS && PWC <= P2S && FT <= RMS, "row strides");
+    // a column-pass item covers row pairs p0 .. p0 + FM/2 - 1, p0 <= PP - FM/2,
+    // and reads row pairs up to p0 + FM/2 + KR - 1
+    static_assert(PP >= FM / 2 && PP + KR <= RP, "column pass reads computed row pairs");
+    static_assert(PWC <= GPS && PW <= P2S && FT <= RMS, "row strides");
     static_assert(US <= 256 && RH <= 256 && (US * 2) % 16 == 0, "TMA box");
     static_assert((NPW - 1) * FM < US && (FM * 2) % 16 == 0, "16-byte raw loads start inside a U row");
     static_assert(SMEM <= 227 * 1024, "shared memory");
     static_assert(RC + 2 <= HP && RC <= HX, "walk and feature circles inside the processed region");
-    static_assert(TH0 * FT * 4 + (fast_threads(TH0) / 32) * 32 * 20 <= SZ_BP,
-                  "candidate list and emission staging fit the dead boxcar region");
+    static_assert(NTK / 32 > 2 * NWO, "stencil warps besides the walkers");
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -307,323 +327,51 @@ __device__ __forceinline__ bool centroid_fixed(const LocParams& p, const P2Acc<G
 
 }  // namespace
 
-template <int KR, int DD, int TH0, int RC>
-__global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
-    locate_fast_kernel(const LocParams p, const MovieBufs b, const __grid_constant__ CUtensorMap tmap, int use_tma,
-                       int frame0) {
-    using G = Geo<KR, DD, TH0, RC>;
-    constexpr int NTK = fast_threads(TH0);
-    constexpr int TAPS = 2 * KR + 1;
-    constexpr int O = G::O;
-    constexpr int HP = G::HP, HX = G::HX;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_fail, s_nc;
-    __shared__ unsigned long long rowmask[TH0];  // columns of the tile row that emit a record
+namespace {
+// Output tile g of a launch: tiles are numbered frame by frame, frame0 first.
+struct FTile {
+    int t, tj, ty0, tx0, TH;
+};
 
-    const int tid = threadIdx.x;
-    const int tile = blockIdx.x;
-    const int t = frame0 + blockIdx.y;
-    const int ti = tile / p.ntx, tj = tile - ti * p.ntx;
-    const int ty0 = ti * TH0, tx0 = tj * FT;
+template <int TH0>
+__device__ __forceinline__ FTile tile_of(const LocParams& p, int frame0, int ntiles, int g) {
+    FTile f;
+    const int fr = g / ntiles, tile = g - fr * ntiles;
+    const int ti = tile / p.ntx;
+    f.t = frame0 + fr;
+    f.tj = tile - ti * p.ntx;
+    f.ty0 = ti * TH0;
+    f.tx0 = f.tj * FT;
+    f.TH = min(TH0, p.H - f.ty0);
+    return f;
+}
+
+__device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+__device__ __forceinline__ void bar_arrive(int id, int n) {
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// ---- 5. walks and emission of tile f, by the walker warps ----
+// The list is walked one candidate per lane, so the walks, the costliest
+// code per candidate, run with full warps.  Lane index c holds list entry q
+// when `have` (read by the caller); list entries c + wstride, c + 2 wstride,
+// ... (candidates beyond one per walker thread) are read from the list here
+// and emitted as pending without a walk (fallback_walk_kernel walks them).
+// Records are ranked within their (row, tile) segment from a per-row bit
+// mask of the columns that emit, which is what finalize_kernel needs; slots
+// come from one atomic per warp.  Named barrier 1 syncs the nwt walker
+// threads.
+template <class G, int RC>
+__device__ __forceinline__ void walk_emit(const LocParams& p, const MovieBufs& b, const FTile& f, const float* P2f,
+                                          const unsigned short* clist, unsigned long long* rowmask, int* stage,
+                                          float4* sfeat, const int2* offs, const float* r2s, const float2* sc,
+                                          int ncand, int c, bool have, int q, int wstride, int nwt) {
     const int H = p.H, W = p.W;
-    const int ry0 = ty0 - HP - KR, rx0 = tx0 - G::L;
-    const int py0 = ty0 - HP, px0 = tx0 - HX;
-    const int TH = min(TH0, H - ty0);
-
-    float2* P2 = (float2*)smem;
-    float2* Gp = (float2*)(smem + G::OFF_GP);
-    float2* Bp = (float2*)(smem + G::OFF_BP);
-    unsigned short* U = (unsigned short*)(smem + G::OFF_U);  // raw tile, row stride US
-    float2* RM2 = Gp;                           // after the column pass
-    int* clist = (int*)Bp;                      // candidate list: the boxcar is dead after the column pass
-    float2* sc = (float2*)(smem + G::OFF_TAB);  // (sin2, cos2) of the d/2 circle
-
-    // ---- 0. stage the raw tile ----
-    if (use_tma) {
-        if (tid == 0) {
-            mbar_init(&bar, 1);
-            s_fail = 0;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            mbar_expect_tx(&bar, (uint32_t)(G::RH * G::US * 2));
-            // tma_withhold (a test of the timeout path) issues no copy: the
-            // barrier then never completes and the bounded wait runs out
-            if (!p.tma_withhold) tma_load_3d(U, &tmap, &bar, rx0, ry0, t);
-            bool done = false;
-            for (int it = 0; it < p.tma_spin && !done; ++it) done = mbar_try_wait(&bar, 0);
-            if (!done) {
-                atomicOr(b.err, ERR_DEVICE_TIMEOUT);
-                s_fail = 1;
-                // give the copy in flight a second bounded wait to land in
-                // this CTA's shared memory before the CTA exits
-                for (int it = 0; it < p.tma_spin && !done; ++it) done = mbar_try_wait(&bar, 0);
-            }
-        }
-        __syncthreads();
-        if (s_fail) return;
-    } else {
-        const unsigned short* fr = (const unsigned short*)b.frames + (size_t)t * H * W;
-        for (int i = tid; i < G::RH * G::US; i += NTK) {
-            const int r = i / G::US, c = i - r * G::US;
-            const int gy = ry0 + r, gx = rx0 + c;
-            unsigned short v = 0;
-            if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(fr + (size_t)gy * W + gx);
-            U[i] = v;
-        }
-        __syncthreads();
-    }
-    if (tid < TH0) rowmask[tid] = 0ull;
-    if (tid == 0) s_nc = 0;
-    int2* offs = (int2*)(smem + G::OFF_TAB + G::K * 8);  // P2 offsets of the d/2 circle by centre parity
-    float* r2s = (float*)(smem + G::OFF_TAB + G::K * 16);
-    if (p.cpu_processed)
-        for (int k = tid; k < G::K; k += NTK) {
-            sc[k] = make_float2(__ldg(b.char_tab + 3 * k + 1), __ldg(b.char_tab + 3 * k + 2));
-            r2s[k] = __ldg(b.char_tab + 3 * k);
-            const int di = __ldg(b.char_off + 2 * k), dj = __ldg(b.char_off + 2 * k + 1);
-            offs[k] = make_int2(((di >> 1) * G::P2S + dj) * 2 + (di & 1),
-                                (((1 + di) >> 1) * G::P2S + dj) * 2 + ((1 + di) & 1));
-        }
-
-    float2 W2[TAPS];
-#pragma unroll
-    for (int j = 0; j < TAPS; ++j) W2[j] = make_float2(p.w[j], p.w[j]);
-    const float2 RN2 = make_float2(p.rn, p.rn), NRKK2 = make_float2(-p.rkk, -p.rkk);
-
-    // ---- 1. row pass (preprocess_rows.wgsl) on row pairs ----
-    for (int it = tid; it < G::RP * G::NPW; it += NTK) {
-        const int q = it / G::RP, pr = it - q * G::RP;
-        const int pc0 = q * FM;
-        // raw rows 2 pr and 2 pr + 1 as exact floats: 0x4B000000 | u is 2^23 + u
-        const uint4* r0 = (const uint4*)(U + (2 * pr) * G::US + pc0);
-        const uint4* r1 = (const uint4*)(U + (2 * pr + 1) * G::US + pc0);
-        float2 v[8 * G::NV];
-#pragma unroll
-        for (int l = 0; l < G::NV; ++l) {
-            const uint4 a4 = r0[l], c4 = r1[l];
-            const unsigned int wa[4] = {a4.x, a4.y, a4.z, a4.w}, wc[4] = {c4.x, c4.y, c4.z, c4.w};
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                const float2 lo = make_float2(__uint_as_float(__byte_perm(wa[h], 0x4B00u, 0x5410)),
-                                              __uint_as_float(__byte_perm(wc[h], 0x4B00u, 0x5410)));
-                const float2 hi = make_float2(__uint_as_float(__byte_perm(wa[h], 0x4B00u, 0x5432)),
-                                              __uint_as_float(__byte_perm(wc[h], 0x4B00u, 0x5432)));
-                v[8 * l + 2 * h] = add2(lo, make_float2(-8388608.f, -8388608.f));
-                v[8 * l + 2 * h + 1] = add2(hi, make_float2(-8388608.f, -8388608.f));
-            }
-        }
-        float2* gd = Gp + pr * G::GPS + pc0;
-        float2* bd = Bp + pr * G::GPS + pc0;
-#pragma unroll
-        for (int m = 0; m < FM; ++m) {
-            float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int j = 0; j < TAPS; ++j) acc = fma2(W2[j], v[m + j], acc);
-            gd[m] = mul2(acc, RN2);  // preprocess_rows.wgsl:52
-        }
-        const int fc0 = rx0 + pc0;  // frame column of v[0]
-        if (fc0 >= 0 && fc0 + FM + 2 * KR - 1 < W) {
-            float2 s = v[0];
-#pragma unroll
-            for (int j = 1; j < TAPS; ++j) s = add2(s, v[j]);
-            bd[0] = s;
-#pragma unroll
-            for (int m = 1; m < FM; ++m) {
-                s = sub2(add2(s, v[m + 2 * KR]), v[m - 1]);
-                bd[m] = s;
-            }
-        } else {
-            // reflect-padded boxcar at the left/right frame edges
-#pragma unroll
-            for (int m = 0; m < FM; ++m) {
-                const int fc = fc0 + m + KR;
-                float2 s = make_float2(0.f, 0.f);
-#pragma unroll
-                for (int j = 0; j < TAPS; ++j) {
-                    const int cc = clampi(reflect_once(fc - KR + j, W) - rx0, 0, G::RW - 1);
-                    s = add2(s, make_float2((float)U[(2 * pr) * G::US + cc], (float)U[(2 * pr + 1) * G::US + cc]));
-                }
-                bd[m] = s;
-            }
-        }
-    }
-    __syncthreads();
-
-    // ---- 2. column pass (preprocess_cols.wgsl) -> P2 ----
-    const float NEG = -CUDART_INF_F;
-    for (int it = tid; it < G::PWC * G::NRQ; it += NTK) {
-        const int rq = it / G::PWC, c = it - rq * G::PWC;
-        const int p0 = rq * (FM / 2);
-        float2 L[FM / 2 + KR], ML[FM / 2 + KR - 1];
-#pragma unroll
-        for (int k = 0; k < FM / 2 + KR; ++k) L[k] = Gp[(p0 + k) * G::GPS + c];
-#pragma unroll
-        for (int k = 0; k < FM / 2 + KR - 1; ++k) ML[k] = make_float2(L[k].y, L[k + 1].x);
-        float2 gq[FM / 2];
-#pragma unroll
-        for (int m = 0; m < FM / 2; ++m) {
-            float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int j = 0; j < TAPS; ++j) acc = fma2(W2[j], (j & 1) ? ML[m + (j >> 1)] : L[m + (j >> 1)], acc);
-            gq[m] = mul2(acc, RN2);
-        }
-        float2 cs[FM / 2];
-        const int fr0 = ry0 + 2 * p0;  // frame row of raw row 2*p0
-        if (fr0 >= 0 && fr0 + FM + 2 * KR - 1 < H) {
-#pragma unroll
-            for (int k = 0; k < FM / 2 + KR; ++k) L[k] = Bp[(p0 + k) * G::GPS + c];
-            // the rows' box sums in scalar: the first window summed in tap
-            // order, each next row's window slid by one row; every partial
-            // sum is an integer below 2^24 (u16 frames), so all orders give
-            // the same bits
-            float b[FM + 2 * KR];
-#pragma unroll
-            for (int k = 0; k < FM / 2 + KR; ++k) { b[2 * k] = L[k].x; b[2 * k + 1] = L[k].y; }
-            float sb[FM];
-            float s0 = b[0];
-#pragma unroll
-            for (int j = 1; j < TAPS; ++j) s0 = s0 + b[j];
-            sb[0] = s0;
-#pragma unroll
-            for (int m = 1; m < FM; ++m) {
-                s0 = s0 + b[m + 2 * KR];
-                s0 = s0 - b[m - 1];
-                sb[m] = s0;
-            }
-#pragma unroll
-            for (int m = 0; m < FM / 2; ++m) cs[m] = make_float2(sb[2 * m], sb[2 * m + 1]);
-        } else {
-            // reflect-padded boxcar at the top/bottom frame edges
-            const float* Bf = (const float*)Bp;
-#pragma unroll
-            for (int m = 0; m < FM / 2; ++m) {
-                float sx = 0.f, sy = 0.f;
-                const int fa = fr0 + 2 * m + KR;  // frame row of the output pair's first row
-#pragma unroll
-                for (int j = 0; j < TAPS; ++j) {
-                    const int ra = clampi(reflect_once(fa - KR + j, H) - ry0, 0, G::RH - 1);
-                    const int rb = clampi(reflect_once(fa + 1 - KR + j, H) - ry0, 0, G::RH - 1);
-                    sx = sx + Bf[(((ra >> 1) * G::GPS + c) << 1) + (ra & 1)];
-                    sy = sy + Bf[(((rb >> 1) * G::GPS + c) << 1) + (rb & 1)];
-                }
-                cs[m] = make_float2(sx, sy);
-            }
-        }
-        const int fc = px0 + c;
-        const bool cin = fc >= 0 && fc < W && c < G::PW;
-        const int fa0 = py0 + 2 * p0;  // frame row of the item's first output
-        const bool all_in = cin && fa0 >= 0 && fa0 + FM - 1 < H;
-#pragma unroll
-        for (int m = 0; m < FM / 2; ++m) {
-            // preprocess_cols.wgsl:54 contracted: fma(-cs, 1/k^2, gauss);
-            // cs * -rkk is exactly -(cs * rkk)
-            const float2 res = fma2(cs[m], NRKK2, gq[m]);
-            // preprocess_cols.wgsl:55-60 clip at 0; res is never NaN or -0
-            // here (u16 frames, non-negative sums), where max equals the
-            // shader's select
-            float2 o;
-            o.x = fmaxf(res.x, 0.f);
-            o.y = fmaxf(res.y, 0.f);
-            if (!all_in) {
-                const int fa = fa0 + 2 * m;
-                if (!(cin && fa >= 0 && fa < H)) o.x = NEG;
-                if (!(cin && fa + 1 >= 0 && fa + 1 < H)) o.y = NEG;
-            }
-            P2[(p0 + m) * G::P2S + c] = o;
-        }
-    }
-    __syncthreads();
-
-    // ---- 3. row max over the dilation window (max_rows.wgsl) ----
-    for (int it = tid; it < G::PP * (FT / FM); it += NTK) {
-        const int q = it / G::PP, pr = it - q * G::PP;
-        const int tc0 = q * FM;
-        const float2* src = P2 + pr * G::P2S + tc0 + HX - O;
-        float vx[FM + DD - 1], vy[FM + DD - 1];
-#pragma unroll
-        for (int i = 0; i < FM + DD - 1; ++i) {
-            const float2 z = src[i];
-            vx[i] = z.x;
-            vy[i] = z.y;
-        }
-        float ox[FM], oy[FM];
-        slide_max<DD, FM>(vx, ox);
-        slide_max<DD, FM>(vy, oy);
-#pragma unroll
-        for (int m = 0; m < FM; ++m) RM2[pr * G::RMS + tc0 + m] = make_float2(ox[m], oy[m]);
-    }
-    __syncthreads();
-
-    // ---- 4. column max vs centre: non-strict local max (walk_cols.wgsl:19-36),
-    //         listed at once: warp w owns tile rows 8 (w / 2) .. + 7 of
-    //         column half w % 2, ballots each row and appends its flagged
-    //         pixels to the CTA list (one shared atomic per warp; the order
-    //         of the list does not matter: records carry their rank) ----
-    constexpr int NW = NTK / 32;
-    static_assert(FT * (TH0 / FM) == NTK && FT == 64, "one column of 8 rows per thread");
-    const int warp = tid >> 5, lane = tid & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    {
-        const int tc = tid % FT, rq = tid / FT;
-        const int tr0 = rq * FM;
-        const int k0 = (tr0 + HP - O) >> 1;  // HP - O is even
-        constexpr int NPR = (FM + DD - 1 + 1) / 2;
-        float vv[2 * NPR];
-#pragma unroll
-        for (int k = 0; k < NPR; ++k) {
-            const float2 z = RM2[(k0 + k) * G::RMS + tc];
-            vv[2 * k] = z.x;
-            vv[2 * k + 1] = z.y;
-        }
-        float v[FM + DD - 1];
-#pragma unroll
-        for (int i = 0; i < FM + DD - 1; ++i) v[i] = vv[i];
-        float cm[FM];
-        slide_max<DD, FM>(v, cm);
-        const float* Pf = (const float*)P2;
-        const bool col_in = tx0 + tc < W;
-        unsigned bal[FM];
-        int nc = 0;
-#pragma unroll
-        for (int m = 0; m < FM; ++m) {
-            const int r = tr0 + m + HP;  // processed row of the centre
-            const float center = Pf[(((r >> 1) * G::P2S + tc + HX) << 1) + (r & 1)];
-            const bool in = col_in && tr0 + m < TH;
-            const bool f = in && cm[m] <= center && !(p.zero_skip && center == 0.f);
-            bal[m] = __ballot_sync(0xffffffffu, f);
-            nc += __popc(bal[m]);
-        }
-        int wbase = 0;
-        if (lane == 0 && nc) wbase = atomicAdd(&s_nc, nc);
-        wbase = __shfl_sync(0xffffffffu, wbase, 0);
-#pragma unroll
-        for (int m = 0; m < FM; ++m) {
-            if ((bal[m] >> lane) & 1u) clist[wbase + __popc(bal[m] & lt)] = (tr0 + m) * FT + tc;
-            wbase += __popc(bal[m]);
-        }
-    }
-    __syncthreads();
-
-    // ---- 5. walks and emission ----
-    // The list is walked one candidate per lane by as few warps as it needs
-    // (the other warps leave: the walks, the costliest code per candidate,
-    // run with full warps and cost the SM's other CTA few issue slots).
-    // Records are ranked within their (row, tile) segment from a per-row
-    // bit mask of the columns that emit, which is what finalize_kernel
-    // needs; slots come from one atomic per warp.  Candidates beyond one per
-    // thread of the CTA are emitted as pending without a walk;
-    // fallback_walk_kernel walks them.
-    const int ncand = s_nc;
-    const int nwalk = min(NW, max(1, (ncand + 31) >> 5));
-    if (warp >= nwalk) return;  // only the named barrier below follows
-    const int wstride = nwalk * 32;
-
-    P2Acc<G> acc{(const float*)P2, py0, px0};
-    const int c = warp * 32 + lane;
-    const bool have = c < ncand;
-    const int q = have ? clist[c] : 0;
+    const int t = f.t, ty0 = f.ty0, tx0 = f.tx0;
+    const int py0 = ty0 - G::HP, px0 = tx0 - G::HX;
+    P2Acc<G> acc{P2f, py0, px0};
     const int tr = q / FT, tc = q - tr * FT;
     const int u0 = ty0 + tr, v0 = tx0 + tc;
     int st = CAND_REJECT;
@@ -672,11 +420,11 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     // atomic's latency overlaps the barrier and the sums below
     int gbase = 0;
     if (lane == 0 && nrec) gbase = atomicAdd(b.fcount + t, nrec);
-    if (nwalk > 1) asm volatile("bar.sync 1, %0;" ::"r"(wstride) : "memory");
+    if (nwt > 32) bar_sync(1, nwt);
     else __syncwarp();
     if (warp == 0)
-        for (int r = lane; r < TH; r += 32)
-            b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + tj] = __popcll(rowmask[r]);
+        for (int r = lane; r < f.TH; r += 32)
+            b.rowcnt[((size_t)t * H + ty0 + r) * p.ntx + f.tj] = __popcll(rowmask[r]);
 
     // emission: the first stride of the list from the walks above, later
     // strides as pending records.  The cpu_processed sums of a stride's
@@ -685,9 +433,6 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     // meanwhile.
     const unsigned short* frame = (const unsigned short*)b.frames + (size_t)t * H * W;
     GRawAcc racc{frame, W};
-    const float* P2f = (const float*)P2;
-    int* stage = (int*)((unsigned char*)Bp + TH0 * FT * 4) + warp * 32;  // after the candidate list
-    float4* sfeat = (float4*)((unsigned char*)Bp + TH0 * FT * 4 + NW * 32 * 4) + warp * 32;
     int roff = 0;
     for (int c0 = 0; c0 < ncand; c0 += wstride) {
         int rq = q, rtr = tr, rtc = tc, rst = st;
@@ -761,6 +506,395 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         roff += ne;
     }
 }
+}  // namespace
+
+// A CTA locates a run of consecutive tiles [g0, g0 + ntl) of the launch.
+// Warps 0 and 1 walk tile k - 1's candidates and emit its records (when it
+// has at most 64) while warps 2.. run tile k's row pass, and, with two
+// processed planes (G::WS), its column pass and row max too: the warps meet
+// only for the column max and the list.  With one plane the walkers hold the
+// plane until the column pass.  A tile with more candidates is walked by as
+// many warps as it needs before the next tile starts.  The next raw tile is
+// copied in as soon as a row pass is done with the current one.  Named
+// barriers: 1 the walker warps, 2 "tile k - 1's list is read" (walkers
+// arrive, the stencil warps wait), 3 all warps before the column max (two
+// planes) or the column pass (one plane), 4 the stencil warps after a
+// staging without TMA, 5 the stencil warps between their phases.  A tile
+// copy that does not land within the bounded wait sets ERR_DEVICE_TIMEOUT;
+// the CTA then issues no further copies, lists no candidates and finishes its
+// run (every barrier is still reached; the host discards the results).
+template <int KR, int DD, int TH0, int RC>
+__global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
+    locate_fast_kernel(const LocParams p, const MovieBufs b, const __grid_constant__ CUtensorMap tmap, int use_tma,
+                       int frame0, int ntiles, int total, int per_cta) {
+    using G = Geo<KR, DD, TH0, RC>;
+    constexpr int NTK = fast_threads(TH0);
+    constexpr int NW = NTK / 32;
+    constexpr int TAPS = 2 * KR + 1;
+    constexpr int O = G::O;
+    constexpr int HP = G::HP, HX = G::HX;
+    constexpr int NWT = NWO * 32;       // walker threads while tiles overlap
+    constexpr int NS = NTK - NWT;       // stencil threads
+    constexpr int PROD = NTK - 32;      // issues the tile copies: a stencil thread
+    // column pass and row max: the stencil warps (two planes) or all warps
+    constexpr int CB = G::WS ? NWT : 0, CN = NTK - CB;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_fail, s_nc;
+    __shared__ unsigned long long rowmask[TH0];  // columns of the tile row that emit a record
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int g0 = blockIdx.x * per_cta;
+    const int ntl = min(per_cta, total - g0);
+    const int H = p.H, W = p.W;
+
+    float2* Gp = (float2*)(smem + G::OFF_GP);
+    float2* Bp = (float2*)(smem + G::OFF_BP);
+    unsigned short* U = (unsigned short*)(smem + G::OFF_U);  // raw tile, row stride US
+    float2* RM2 = Gp;                                         // after the column pass
+    unsigned short* clist = (unsigned short*)Bp;  // candidate list: the boxcar is dead after the column pass
+    float2* sc = (float2*)(smem + G::OFF_TAB);    // (sin2, cos2) of the d/2 circle
+    int2* offs = (int2*)(smem + G::OFF_TAB + G::K * 8);  // P2 offsets of the d/2 circle by centre parity
+    float* r2s = (float*)(smem + G::OFF_TAB + G::K * 16);
+    // emission staging of the walker warps: their own region while the
+    // next tile's row pass fills the boxcar rows, else after the list
+    int* stage_ov = (int*)(smem + G::OFF_STG);
+    float4* sfeat_ov = (float4*)(smem + G::OFF_STG + NWO * 32 * 4);
+    int* stage_bp = (int*)((unsigned char*)Bp + TH0 * FT * 2);
+    float4* sfeat_bp = (float4*)((unsigned char*)Bp + TH0 * FT * 2 + NW * 32 * 4);
+
+    // ---- set-up: the first tile's copy, tables ----
+    if (tid == 0) { s_fail = 0; s_nc = 0; }
+    if (tid < TH0) rowmask[tid] = 0ull;
+    if (use_tma && tid == PROD) {
+        mbar_init(&bar, 1);
+        const FTile f = tile_of<TH0>(p, frame0, ntiles, g0);
+        mbar_expect_tx(&bar, (uint32_t)(G::RH * G::US * 2));
+        // tma_withhold (a test of the timeout path) issues no copy: the
+        // barrier then never completes and the bounded wait runs out
+        if (!p.tma_withhold) tma_load_3d(U, &tmap, &bar, f.tx0 - G::L, f.ty0 - HP - KR, f.t);
+    }
+    if (p.cpu_processed)
+        for (int k = tid; k < G::K; k += NTK) {
+            sc[k] = make_float2(__ldg(b.char_tab + 3 * k + 1), __ldg(b.char_tab + 3 * k + 2));
+            r2s[k] = __ldg(b.char_tab + 3 * k);
+            const int di = __ldg(b.char_off + 2 * k), dj = __ldg(b.char_off + 2 * k + 1);
+            offs[k] = make_int2(((di >> 1) * G::P2S + dj) * 2 + (di & 1),
+                                (((1 + di) >> 1) * G::P2S + dj) * 2 + ((1 + di) & 1));
+        }
+    __syncthreads();
+
+    float2 W2[TAPS];
+#pragma unroll
+    for (int j = 0; j < TAPS; ++j) W2[j] = make_float2(p.w[j], p.w[j]);
+    const float2 RN2 = make_float2(p.rn, p.rn), NRKK2 = make_float2(-p.rkk, -p.rkk);
+    const float NEG = -CUDART_INF_F;
+
+    FTile prev{};  // tile k - 1, walked at the top of iteration k
+    int last = 0;  // the last tile whose copy was issued (copy-issuing thread)
+    for (int k = 0; k <= ntl; ++k) {
+        if (k > 0) {
+            const int ncand = s_nc;
+            const bool more = k < ntl;
+            const float* P2w = (const float*)(smem + (G::WS ? ((k - 1) & 1) * G::SZ_P2 : 0));
+            // at most 64 candidates: the two walker warps take halves of the
+            // list, and the stencil warps go on once every walker has read
+            // its entry; a crowded tile is walked by warps [0, nwalk), one
+            // candidate per thread, before the next tile starts
+            const bool ov = ncand <= NWT;
+            const int nwt = ov ? NWT : min(NW, (ncand + 31) >> 5) * 32;
+            if (tid < nwt) {
+                const int h = (ncand + 1) >> 1;
+                const int c = !ov ? tid : warp == 0 ? lane : h + lane;
+                const bool have = !ov ? c < ncand : warp == 0 ? lane < h : h + lane < ncand;
+                const int q = have ? clist[c] : 0;
+                if (ov && more) bar_arrive(2, NTK);  // the list (and s_nc) may be overwritten
+                walk_emit<G, RC>(p, b, prev, P2w, clist, rowmask, (ov ? stage_ov : stage_bp) + warp * 32,
+                                 (ov ? sfeat_ov : sfeat_bp) + warp * 32, offs, r2s, sc, ncand, c, have, q, nwt, nwt);
+                if (!more) break;
+                if (nwt > 32) bar_sync(1, nwt);  // every walker reads rowmask until its last record
+                else __syncwarp();
+                for (int r = tid; r < TH0; r += nwt) rowmask[r] = 0ull;
+                if (!ov) bar_sync(2, NTK);
+            } else {
+                if (!more) break;
+                bar_sync(2, NTK);
+            }
+            if (tid == PROD) s_nc = 0;  // every thread has read it (barrier 2)
+        }
+        const FTile f = tile_of<TH0>(p, frame0, ntiles, g0 + k);
+        const int ry0 = f.ty0 - HP - KR, rx0 = f.tx0 - G::L;
+        const int py0 = f.ty0 - HP, px0 = f.tx0 - HX;
+        float2* P2 = (float2*)(smem + (G::WS ? (k & 1) * G::SZ_P2 : 0));
+        if (warp >= NWO) {
+            const int stid = tid - NWT;
+            // ---- 0. the raw tile ----
+            if (use_tma) {
+                bool done = false;
+                for (int it = 0; it < p.tma_spin && !done && !*(volatile int*)&s_fail; ++it)
+                    done = mbar_try_wait(&bar, k & 1);
+                if (!done && !*(volatile int*)&s_fail) {
+                    atomicOr(b.err, ERR_DEVICE_TIMEOUT);
+                    s_fail = 1;
+                }
+            } else {
+                const unsigned short* fr = (const unsigned short*)b.frames + (size_t)f.t * H * W;
+                for (int i = stid; i < G::RH * G::US; i += NS) {
+                    const int r = i / G::US, c = i - r * G::US;
+                    const int gy = ry0 + r, gx = rx0 + c;
+                    unsigned short v = 0;
+                    if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(fr + (size_t)gy * W + gx);
+                    U[i] = v;
+                }
+                bar_sync(4, NS);
+            }
+
+            // ---- 1. row pass (preprocess_rows.wgsl) on row pairs ----
+            for (int it = stid; it < G::RP * G::NPW; it += NS) {
+                const int q = it / G::RP, pr = it - q * G::RP;
+                const int pc0 = q * FM;
+                // raw rows 2 pr and 2 pr + 1 as exact floats: 0x4B000000 | u is 2^23 + u
+                const uint4* r0 = (const uint4*)(U + (2 * pr) * G::US + pc0);
+                const uint4* r1 = (const uint4*)(U + (2 * pr + 1) * G::US + pc0);
+                float2 v[8 * G::NV];
+#pragma unroll
+                for (int l = 0; l < G::NV; ++l) {
+                    const uint4 a4 = r0[l], c4 = r1[l];
+                    const unsigned int wa[4] = {a4.x, a4.y, a4.z, a4.w}, wc[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) {
+                        const float2 lo = make_float2(__uint_as_float(__byte_perm(wa[h], 0x4B00u, 0x5410)),
+                                                      __uint_as_float(__byte_perm(wc[h], 0x4B00u, 0x5410)));
+                        const float2 hi = make_float2(__uint_as_float(__byte_perm(wa[h], 0x4B00u, 0x5432)),
+                                                      __uint_as_float(__byte_perm(wc[h], 0x4B00u, 0x5432)));
+                        v[8 * l + 2 * h] = add2(lo, make_float2(-8388608.f, -8388608.f));
+                        v[8 * l + 2 * h + 1] = add2(hi, make_float2(-8388608.f, -8388608.f));
+                    }
+                }
+                float2* gd = Gp + pr * G::GPS + pc0;
+                float2* bd = Bp + pr * G::GPS + pc0;
+#pragma unroll
+                for (int m = 0; m < FM; ++m) {
+                    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int j = 0; j < TAPS; ++j) acc = fma2(W2[j], v[m + j], acc);
+                    gd[m] = mul2(acc, RN2);  // preprocess_rows.wgsl:52
+                }
+                const int fc0 = rx0 + pc0;  // frame column of v[0]
+                if (fc0 >= 0 && fc0 + FM + 2 * KR - 1 < W) {
+                    float2 s = v[0];
+#pragma unroll
+                    for (int j = 1; j < TAPS; ++j) s = add2(s, v[j]);
+                    bd[0] = s;
+#pragma unroll
+                    for (int m = 1; m < FM; ++m) {
+                        s = sub2(add2(s, v[m + 2 * KR]), v[m - 1]);
+                        bd[m] = s;
+                    }
+                } else {
+                    // reflect-padded boxcar at the left/right frame edges
+#pragma unroll
+                    for (int m = 0; m < FM; ++m) {
+                        const int fc = fc0 + m + KR;
+                        float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int j = 0; j < TAPS; ++j) {
+                            const int cc = clampi(reflect_once(fc - KR + j, W) - rx0, 0, G::RW - 1);
+                            s = add2(s, make_float2((float)U[(2 * pr) * G::US + cc],
+                                                    (float)U[(2 * pr + 1) * G::US + cc]));
+                        }
+                        bd[m] = s;
+                    }
+                }
+            }
+        }
+        if (G::WS) {
+            if (warp >= NWO) bar_sync(5, NS);
+        } else {
+            bar_sync(3, NTK);  // the walkers of tile k - 1 arrive after their records
+        }
+        // the raw tile is read: the next tile's copy lands during this one
+        if (use_tma && tid == PROD && k + 1 < ntl && !s_fail) {
+            const FTile n = tile_of<TH0>(p, frame0, ntiles, g0 + k + 1);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&bar, (uint32_t)(G::RH * G::US * 2));
+            if (!p.tma_withhold) tma_load_3d(U, &tmap, &bar, n.tx0 - G::L, n.ty0 - HP - KR, n.t);
+            last = k + 1;
+        }
+
+        if (tid >= CB) {
+            const int ctid = tid - CB;
+            // ---- 2. column pass (preprocess_cols.wgsl) -> P2 ----
+            // item rq of a column covers row pairs p0 .. p0 + FM/2 - 1; the
+            // last one is moved up to end at the last processed row pair
+            // (the rows it shares with the item before come out the same)
+            for (int it = ctid; it < G::PW * G::NRQ; it += CN) {
+                const int rq = it / G::PW, c = it - rq * G::PW;
+                const int p0 = min(rq * (FM / 2), G::PP - FM / 2);
+                float2 L[FM / 2 + KR], ML[FM / 2 + KR - 1];
+#pragma unroll
+                for (int k2 = 0; k2 < FM / 2 + KR; ++k2) L[k2] = Gp[(p0 + k2) * G::GPS + c];
+#pragma unroll
+                for (int k2 = 0; k2 < FM / 2 + KR - 1; ++k2) ML[k2] = make_float2(L[k2].y, L[k2 + 1].x);
+                float2 gq[FM / 2];
+#pragma unroll
+                for (int m = 0; m < FM / 2; ++m) {
+                    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int j = 0; j < TAPS; ++j)
+                        acc = fma2(W2[j], (j & 1) ? ML[m + (j >> 1)] : L[m + (j >> 1)], acc);
+                    gq[m] = mul2(acc, RN2);
+                }
+                float2 cs[FM / 2];
+                const int fr0 = ry0 + 2 * p0;  // frame row of raw row 2*p0
+                if (fr0 >= 0 && fr0 + FM + 2 * KR - 1 < H) {
+#pragma unroll
+                    for (int k2 = 0; k2 < FM / 2 + KR; ++k2) L[k2] = Bp[(p0 + k2) * G::GPS + c];
+                    // the rows' box sums in scalar: the first window summed in tap
+                    // order, each next row's window slid by one row; every partial
+                    // sum is an integer below 2^24 (u16 frames), so all orders give
+                    // the same bits
+                    float bsum[FM + 2 * KR];
+#pragma unroll
+                    for (int k2 = 0; k2 < FM / 2 + KR; ++k2) { bsum[2 * k2] = L[k2].x; bsum[2 * k2 + 1] = L[k2].y; }
+                    float sb[FM];
+                    float s0 = bsum[0];
+#pragma unroll
+                    for (int j = 1; j < TAPS; ++j) s0 = s0 + bsum[j];
+                    sb[0] = s0;
+#pragma unroll
+                    for (int m = 1; m < FM; ++m) {
+                        s0 = s0 + bsum[m + 2 * KR];
+                        s0 = s0 - bsum[m - 1];
+                        sb[m] = s0;
+                    }
+#pragma unroll
+                    for (int m = 0; m < FM / 2; ++m) cs[m] = make_float2(sb[2 * m], sb[2 * m + 1]);
+                } else {
+                    // reflect-padded boxcar at the top/bottom frame edges
+                    const float* Bf = (const float*)Bp;
+#pragma unroll
+                    for (int m = 0; m < FM / 2; ++m) {
+                        float sx = 0.f, sy = 0.f;
+                        const int fa = fr0 + 2 * m + KR;  // frame row of the output pair's first row
+#pragma unroll
+                        for (int j = 0; j < TAPS; ++j) {
+                            const int ra = clampi(reflect_once(fa - KR + j, H) - ry0, 0, G::RH - 1);
+                            const int rb = clampi(reflect_once(fa + 1 - KR + j, H) - ry0, 0, G::RH - 1);
+                            sx = sx + Bf[(((ra >> 1) * G::GPS + c) << 1) + (ra & 1)];
+                            sy = sy + Bf[(((rb >> 1) * G::GPS + c) << 1) + (rb & 1)];
+                        }
+                        cs[m] = make_float2(sx, sy);
+                    }
+                }
+                const int fc = px0 + c;
+                const bool cin = fc >= 0 && fc < W;
+                const int fa0 = py0 + 2 * p0;  // frame row of the item's first output
+                const bool all_in = cin && fa0 >= 0 && fa0 + FM - 1 < H;
+#pragma unroll
+                for (int m = 0; m < FM / 2; ++m) {
+                    // preprocess_cols.wgsl:54 contracted: fma(-cs, 1/k^2, gauss);
+                    // cs * -rkk is exactly -(cs * rkk)
+                    const float2 res = fma2(cs[m], NRKK2, gq[m]);
+                    // preprocess_cols.wgsl:55-60 clip at 0; res is never NaN or -0
+                    // here (u16 frames, non-negative sums), where max equals the
+                    // shader's select
+                    float2 o;
+                    o.x = fmaxf(res.x, 0.f);
+                    o.y = fmaxf(res.y, 0.f);
+                    if (!all_in) {
+                        const int fa = fa0 + 2 * m;
+                        if (!(cin && fa >= 0 && fa < H)) o.x = NEG;
+                        if (!(cin && fa + 1 >= 0 && fa + 1 < H)) o.y = NEG;
+                    }
+                    P2[(p0 + m) * G::P2S + c] = o;
+                }
+            }
+            if (G::WS) bar_sync(5, NS);
+            else __syncthreads();
+
+            // ---- 3. row max over the dilation window (max_rows.wgsl) ----
+            for (int it = ctid; it < G::PP * (FT / FM); it += CN) {
+                const int q = it / G::PP, pr = it - q * G::PP;
+                const int tc0 = q * FM;
+                const float2* src = P2 + pr * G::P2S + tc0 + HX - O;
+                float vx[FM + DD - 1], vy[FM + DD - 1];
+#pragma unroll
+                for (int i = 0; i < FM + DD - 1; ++i) {
+                    const float2 z = src[i];
+                    vx[i] = z.x;
+                    vy[i] = z.y;
+                }
+                float ox[FM], oy[FM];
+                slide_max<DD, FM>(vx, ox);
+                slide_max<DD, FM>(vy, oy);
+#pragma unroll
+                for (int m = 0; m < FM; ++m) RM2[pr * G::RMS + tc0 + m] = make_float2(ox[m], oy[m]);
+            }
+        }
+        if (G::WS) bar_sync(3, NTK);  // the walkers of tile k - 1 arrive after their records
+        else __syncthreads();
+
+        // ---- 4. column max vs centre: non-strict local max (walk_cols.wgsl:19-36),
+        //         listed at once: warp w owns tile rows 8 (w / 2) .. + 7 of
+        //         column half w % 2, ballots each row and appends its flagged
+        //         pixels to the CTA list (one shared atomic per warp; the order
+        //         of the list does not matter: records carry their rank) ----
+        static_assert(FT * (TH0 / FM) == NTK && FT == 64, "one column of 8 rows per thread");
+        {
+            const int tc = tid % FT, rq = tid / FT;
+            const int tr0 = rq * FM;
+            const int k0 = (tr0 + HP - O) >> 1;  // HP - O is even
+            constexpr int NPR = (FM + DD - 1 + 1) / 2;
+            float vv[2 * NPR];
+#pragma unroll
+            for (int k2 = 0; k2 < NPR; ++k2) {
+                const float2 z = RM2[(k0 + k2) * G::RMS + tc];
+                vv[2 * k2] = z.x;
+                vv[2 * k2 + 1] = z.y;
+            }
+            float v[FM + DD - 1];
+#pragma unroll
+            for (int i = 0; i < FM + DD - 1; ++i) v[i] = vv[i];
+            float cm[FM];
+            slide_max<DD, FM>(v, cm);
+            const float* Pf = (const float*)P2;
+            // a tile whose copy ran out of its wait lists nothing
+            const bool col_in = f.tx0 + tc < W && !*(volatile int*)&s_fail;
+            unsigned bal[FM];
+            int nc = 0;
+#pragma unroll
+            for (int m = 0; m < FM; ++m) {
+                const int r = tr0 + m + HP;  // processed row of the centre
+                const float center = Pf[(((r >> 1) * G::P2S + tc + HX) << 1) + (r & 1)];
+                const bool in = col_in && tr0 + m < f.TH;
+                const bool fl = in && cm[m] <= center && !(p.zero_skip && center == 0.f);
+                bal[m] = __ballot_sync(0xffffffffu, fl);
+                nc += __popc(bal[m]);
+            }
+            int wbase = 0;
+            if (lane == 0 && nc) wbase = atomicAdd(&s_nc, nc);
+            wbase = __shfl_sync(0xffffffffu, wbase, 0);
+#pragma unroll
+            for (int m = 0; m < FM; ++m) {
+                if ((bal[m] >> lane) & 1u)
+                    clist[wbase + __popc(bal[m] & lt)] = (unsigned short)((tr0 + m) * FT + tc);
+                wbase += __popc(bal[m]);
+            }
+        }
+        __syncthreads();
+        prev = f;
+    }
+    // a copy that ran out of the bounded wait gets a second one to land in
+    // this CTA's shared memory before the CTA exits (no copy is issued after
+    // a timeout, so only the last one can be in flight)
+    if (use_tma && tid == PROD && s_fail) {
+        bool done = false;
+        for (int it = 0; it < p.tma_spin && !done; ++it) done = mbar_try_wait(&bar, last & 1);
+    }
+}
 
 namespace {
 // TMA descriptor over the movie (u16, dims W x H x T) with a box of the raw
@@ -802,10 +936,27 @@ bool fast_supported(int kr, int dd, int rc, int diameter) {
     return false;
 }
 
-// Launches the specialised kernel over frames [frame0, frame0 + grid.y).
-// *used_tma reports whether the raw tiles were staged by TMA.
+// Tiles per CTA of a launch of `total` tiles: runs of up to 8 consecutive
+// tiles (a run overlaps each tile's walks with the next tile's row pass and
+// prefetches the next raw tile), as long as the launch keeps about four
+// waves of CTAs; p.tiles_per_cta > 0 sets it.
+int fast_tiles_per_cta(const LocParams& p, int total, int th) {
+    if (p.tiles_per_cta > 0) return p.tiles_per_cta;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int slots = sms * (th == 32 ? 4 : 2);
+    return std::max(1, std::min(8, total / (4 * slots)));
+}
+
+// Launches the specialised kernel over frames [frame0, frame0 + grid.y),
+// grid.x tiles per frame.  *used_tma reports whether the raw tiles were
+// staged by TMA.
 cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaStream_t st, const LocParams& p,
                                const MovieBufs& b, int T, int frame0, int* used_tma) {
+    const long long total = (long long)grid.x * grid.y;
+    if (total <= 0 || total > (1LL << 30)) return cudaErrorInvalidValue;
+    const int per = fast_tiles_per_cta(p, (int)total, th);
+    const unsigned nblk = (unsigned)((total + per - 1) / per);
 #define GT_FAST_LAUNCH(KR, DD, RC, TH)                                                                  \
     {                                                                                                   \
         using G = Geo<KR, DD, TH, RC>;                                                                  \
@@ -816,7 +967,8 @@ cudaError_t launch_locate_fast(int kr, int dd, int rc, int th, dim3 grid, cudaSt
         cudaError_t e = cudaFuncSetAttribute(locate_fast_kernel<KR, DD, TH, RC>,                         \
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);      \
         if (e != cudaSuccess) return e;                                                                 \
-        locate_fast_kernel<KR, DD, TH, RC><<<grid, fast_threads(TH), G::SMEM, st>>>(p, b, map, tma, frame0); \
+        locate_fast_kernel<KR, DD, TH, RC><<<nblk, fast_threads(TH), G::SMEM, st>>>(p, b, map, tma, frame0, \
+                                                                                   (int)grid.x, (int)total, per); \
         return cudaGetLastError();                                                                      \
     }
 #define GT_FAST_CASE(KR, DD, RC)                                                                        \
