@@ -682,30 +682,54 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
                     for (int j = 0; j < TAPS; ++j) acc = fma2(W2[j], v[m + j], acc);
                     gd[m] = mul2(acc, RN2);  // preprocess_rows.wgsl:52
                 }
-                const int fc0 = rx0 + pc0;  // frame column of v[0]
-                if (fc0 >= 0 && fc0 + FM + 2 * KR - 1 < W) {
-                    float2 s = v[0];
+                // boxcar over the zero-filled raw tile; the columns whose
+                // reflect-padded window differs are redone below
+                float2 s = v[0];
 #pragma unroll
-                    for (int j = 1; j < TAPS; ++j) s = add2(s, v[j]);
-                    bd[0] = s;
+                for (int j = 1; j < TAPS; ++j) s = add2(s, v[j]);
+                bd[0] = s;
 #pragma unroll
-                    for (int m = 1; m < FM; ++m) {
-                        s = sub2(add2(s, v[m + 2 * KR]), v[m - 1]);
-                        bd[m] = s;
+                for (int m = 1; m < FM; ++m) {
+                    s = sub2(add2(s, v[m + 2 * KR]), v[m - 1]);
+                    bd[m] = s;
+                }
+            }
+            // ---- 1b. reflect-padded boxcar at the frame edges (preprocess_rows.wgsl:34-41,
+            //          preprocess_cols.wgsl:36-43), edge tiles only.  Boxcar column c is
+            //          centred on frame column rx0 + KR + c and raw row r is frame row
+            //          ry0 + r.  (h) the in-frame columns within KR of the left or right
+            //          edge are summed over reflected raw columns; (v) then each raw row
+            //          within KR outside the top or bottom edge takes the boxcar row of
+            //          its reflected row, so that the column pass's running sums give the
+            //          reflect-padded vertical sums.  All sums are integers below 2^24,
+            //          exact in any order. ----
+            {
+                float* Bf = (float*)Bp;
+                const int cl0 = max(0, rx0 + KR), cl1 = min(KR, rx0 + KR + G::PWC);
+                const int cr0 = max(W - KR, rx0 + KR), cr1 = min(W, rx0 + KR + G::PWC);
+                const int nl = max(0, cl1 - cl0), nh = nl + max(0, cr1 - cr0);
+                const int rt0 = max(0, -KR - ry0), rt1 = max(rt0, min(G::RH, -ry0));
+                const int rb0 = max(0, H - ry0), rb1 = max(rb0, min(G::RH, H + KR - ry0));
+                const int nt = rt1 - rt0, nv = nt + (rb1 - rb0);
+                if (nh + nv > 0) bar_sync(5, NS);  // the row pass is done
+                if (nh > 0) {
+                    for (int i = stid; i < nh * G::RH; i += NS) {
+                        const int j = i / G::RH, r = i - j * G::RH;
+                        const int fc = j < nl ? cl0 + j : cr0 + (j - nl);
+                        float sum = 0.f;
+#pragma unroll
+                        for (int t2 = 0; t2 < TAPS; ++t2)
+                            sum = sum + (float)U[r * G::US + clampi(reflect_once(fc - KR + t2, W) - rx0, 0, G::RW - 1)];
+                        Bf[(((r >> 1) * G::GPS + (fc - rx0 - KR)) << 1) + (r & 1)] = sum;
                     }
-                } else {
-                    // reflect-padded boxcar at the left/right frame edges
-#pragma unroll
-                    for (int m = 0; m < FM; ++m) {
-                        const int fc = fc0 + m + KR;
-                        float2 s = make_float2(0.f, 0.f);
-#pragma unroll
-                        for (int j = 0; j < TAPS; ++j) {
-                            const int cc = clampi(reflect_once(fc - KR + j, W) - rx0, 0, G::RW - 1);
-                            s = add2(s, make_float2((float)U[(2 * pr) * G::US + cc],
-                                                    (float)U[(2 * pr + 1) * G::US + cc]));
-                        }
-                        bd[m] = s;
+                    if (nv > 0) bar_sync(5, NS);
+                }
+                if (nv > 0) {
+                    for (int i = stid; i < nv * G::PWC; i += NS) {
+                        const int k2 = i / G::PWC, c = i - k2 * G::PWC;
+                        const int r = k2 < nt ? rt0 + k2 : rb0 + (k2 - nt);
+                        const int rs = clampi(reflect_once(ry0 + r, H) - ry0, 0, G::RH - 1);  // an in-frame row
+                        Bf[(((r >> 1) * G::GPS + c) << 1) + (r & 1)] = Bf[(((rs >> 1) * G::GPS + c) << 1) + (rs & 1)];
                     }
                 }
             }
@@ -747,15 +771,14 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
                         acc = fma2(W2[j], (j & 1) ? ML[m + (j >> 1)] : L[m + (j >> 1)], acc);
                     gq[m] = mul2(acc, RN2);
                 }
+                // the rows' box sums in scalar: the first window summed in tap
+                // order, each next row's window slid by one row; every partial
+                // sum is an integer below 2^24 (u16 frames), so all orders give
+                // the same bits
                 float2 cs[FM / 2];
-                const int fr0 = ry0 + 2 * p0;  // frame row of raw row 2*p0
-                if (fr0 >= 0 && fr0 + FM + 2 * KR - 1 < H) {
+                {
 #pragma unroll
                     for (int k2 = 0; k2 < FM / 2 + KR; ++k2) L[k2] = Bp[(p0 + k2) * G::GPS + c];
-                    // the rows' box sums in scalar: the first window summed in tap
-                    // order, each next row's window slid by one row; every partial
-                    // sum is an integer below 2^24 (u16 frames), so all orders give
-                    // the same bits
                     float bsum[FM + 2 * KR];
 #pragma unroll
                     for (int k2 = 0; k2 < FM / 2 + KR; ++k2) { bsum[2 * k2] = L[k2].x; bsum[2 * k2 + 1] = L[k2].y; }
@@ -772,27 +795,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
                     }
 #pragma unroll
                     for (int m = 0; m < FM / 2; ++m) cs[m] = make_float2(sb[2 * m], sb[2 * m + 1]);
-                } else {
-                    // reflect-padded boxcar at the top/bottom frame edges
-                    const float* Bf = (const float*)Bp;
-#pragma unroll
-                    for (int m = 0; m < FM / 2; ++m) {
-                        float sx = 0.f, sy = 0.f;
-                        const int fa = fr0 + 2 * m + KR;  // frame row of the output pair's first row
-#pragma unroll
-                        for (int j = 0; j < TAPS; ++j) {
-                            const int ra = clampi(reflect_once(fa - KR + j, H) - ry0, 0, G::RH - 1);
-                            const int rb = clampi(reflect_once(fa + 1 - KR + j, H) - ry0, 0, G::RH - 1);
-                            sx = sx + Bf[(((ra >> 1) * G::GPS + c) << 1) + (ra & 1)];
-                            sy = sy + Bf[(((rb >> 1) * G::GPS + c) << 1) + (rb & 1)];
-                        }
-                        cs[m] = make_float2(sx, sy);
-                    }
                 }
-                const int fc = px0 + c;
-                const bool cin = fc >= 0 && fc < W;
-                const int fa0 = py0 + 2 * p0;  // frame row of the item's first output
-                const bool all_in = cin && fa0 >= 0 && fa0 + FM - 1 < H;
 #pragma unroll
                 for (int m = 0; m < FM / 2; ++m) {
                     // preprocess_cols.wgsl:54 contracted: fma(-cs, 1/k^2, gauss);
@@ -800,20 +803,36 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
                     const float2 res = fma2(cs[m], NRKK2, gq[m]);
                     // preprocess_cols.wgsl:55-60 clip at 0; res is never NaN or -0
                     // here (u16 frames, non-negative sums), where max equals the
-                    // shader's select
+                    // shader's select; positions outside the frame take -inf below
                     float2 o;
                     o.x = fmaxf(res.x, 0.f);
                     o.y = fmaxf(res.y, 0.f);
-                    if (!all_in) {
-                        const int fa = fa0 + 2 * m;
-                        if (!(cin && fa >= 0 && fa < H)) o.x = NEG;
-                        if (!(cin && fa + 1 >= 0 && fa + 1 < H)) o.y = NEG;
-                    }
                     P2[(p0 + m) * G::P2S + c] = o;
                 }
             }
             if (G::WS) bar_sync(5, NS);
             else __syncthreads();
+            // ---- 2b. processed positions outside the frame take -inf (edge
+            //          tiles only): rows above and below the frame, then
+            //          columns left and right of it ----
+            if (py0 < 0 || px0 < 0 || py0 + G::PH > H || px0 + G::PW > W) {
+                float* Pf = (float*)P2;
+                const int ra = min(G::PH, max(0, -py0)), rb = max(ra, min(G::PH, H - py0));
+                const int ca = min(G::PW, max(0, -px0)), cb = max(ca, min(G::PW, W - px0));
+                const int nrow = ra + (G::PH - rb), ncol = ca + (G::PW - cb);
+                for (int i = ctid; i < nrow * G::PW; i += CN) {
+                    const int k2 = i / G::PW, c = i - k2 * G::PW;
+                    const int r = k2 < ra ? k2 : rb + (k2 - ra);
+                    Pf[(((r >> 1) * G::P2S + c) << 1) + (r & 1)] = NEG;
+                }
+                for (int i = ctid; i < ncol * G::PH; i += CN) {
+                    const int k2 = i / G::PH, r = i - k2 * G::PH;
+                    const int c = k2 < ca ? k2 : cb + (k2 - ca);
+                    Pf[(((r >> 1) * G::P2S + c) << 1) + (r & 1)] = NEG;
+                }
+                if (G::WS) bar_sync(5, NS);
+                else __syncthreads();
+            }
 
             // ---- 3. row max over the dilation window (max_rows.wgsl) ----
             for (int it = ctid; it < G::PP * (FT / FM); it += CN) {
