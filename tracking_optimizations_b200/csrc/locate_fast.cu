@@ -47,9 +47,13 @@ constexpr int FNT = 256;  // threads of a 32-row tile
 // output row) keep 16 warps per SM slot at 2 CTAs per SM
 __host__ __device__ constexpr int fast_threads(int th) { return th == 32 ? FNT : 2 * FNT; }
 constexpr int FM = 8;     // outputs per thread item
-// walker warps of a run of tiles: at most this many walk a tile while the
-// other warps start the next one
-constexpr int NWO = 2;
+// Walker warps of a run of tiles (64-row tiles: 2 of 16 warps, 32-row
+// tiles: 2 of 8): they walk a tile of at most 32 NWO candidates while the
+// other warps start the next one.
+#ifndef GT_WALKERS64
+#define GT_WALKERS64 2
+#endif
+__host__ __device__ constexpr int walker_warps(int th) { return th == 32 ? 2 : GT_WALKERS64; }
 
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int round8(int x) { return (x + 7) / 8 * 8; }
@@ -101,6 +105,7 @@ struct Geo {
     static constexpr int SZ_BP = align128(cmax(RP * GPS * 8, TH0 * FT * 2 + (NTK / 32) * 32 * 20));
     static constexpr int K = circle_size(RC);
     static constexpr int SZ_TAB = align128(K * 20);  // (sin2, cos2), P2 offsets by parity, r2
+    static constexpr int NWO = walker_warps(TH0);
     static constexpr int SZ_STG = align128(NWO * 32 * 20);  // emission staging of the overlapping walkers
     static constexpr int SMEM1 = SZ_P2 + SZ_GP + SZ_BP + SZ_U + SZ_TAB + SZ_STG;
     // Two processed planes (the walkers read the previous tile's while the
@@ -346,6 +351,24 @@ __device__ __forceinline__ FTile tile_of(const LocParams& p, int frame0, int nti
     return f;
 }
 
+// The tile after f in launch order, without divisions.
+template <int TH0>
+__device__ __forceinline__ FTile next_tile(const LocParams& p, FTile f) {
+    f.tj += 1;
+    f.tx0 += FT;
+    if (f.tj == p.ntx) {
+        f.tj = 0;
+        f.tx0 = 0;
+        f.ty0 += TH0;
+        if (f.ty0 >= p.H) {
+            f.ty0 = 0;
+            f.t += 1;
+        }
+    }
+    f.TH = min(TH0, p.H - f.ty0);
+    return f;
+}
+
 __device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 __device__ __forceinline__ void bar_arrive(int id, int n) {
     asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
@@ -533,6 +556,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     constexpr int TAPS = 2 * KR + 1;
     constexpr int O = G::O;
     constexpr int HP = G::HP, HX = G::HX;
+    constexpr int NWO = G::NWO;
     constexpr int NWT = NWO * 32;       // walker threads while tiles overlap
     constexpr int NS = NTK - NWT;       // stencil threads
     constexpr int PROD = NTK - 32;      // issues the tile copies: a stencil thread
@@ -545,7 +569,6 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const unsigned lt = (1u << lane) - 1u;
     const int g0 = blockIdx.x * per_cta;
     const int ntl = min(per_cta, total - g0);
     const int H = p.H, W = p.W;
@@ -593,22 +616,23 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
     const float NEG = -CUDART_INF_F;
 
     FTile prev{};  // tile k - 1, walked at the top of iteration k
+    FTile f = tile_of<TH0>(p, frame0, ntiles, g0);  // tile k
     int last = 0;  // the last tile whose copy was issued (copy-issuing thread)
     for (int k = 0; k <= ntl; ++k) {
         if (k > 0) {
             const int ncand = s_nc;
             const bool more = k < ntl;
             const float* P2w = (const float*)(smem + (G::WS ? ((k - 1) & 1) * G::SZ_P2 : 0));
-            // at most 64 candidates: the two walker warps take halves of the
-            // list, and the stencil warps go on once every walker has read
-            // its entry; a crowded tile is walked by warps [0, nwalk), one
-            // candidate per thread, before the next tile starts
+            // at most 32 NWO candidates: the walker warps take equal shares
+            // of the list, and the stencil warps go on once every walker has
+            // read its entry; a crowded tile is walked by warps [0, nwalk),
+            // one candidate per thread, before the next tile starts
             const bool ov = ncand <= NWT;
             const int nwt = ov ? NWT : min(NW, (ncand + 31) >> 5) * 32;
             if (tid < nwt) {
-                const int h = (ncand + 1) >> 1;
-                const int c = !ov ? tid : warp == 0 ? lane : h + lane;
-                const bool have = !ov ? c < ncand : warp == 0 ? lane < h : h + lane < ncand;
+                const int h = (ncand + NWO - 1) / NWO;
+                const int c = ov ? warp * h + lane : tid;
+                const bool have = ov ? lane < h && c < ncand : c < ncand;
                 const int q = have ? clist[c] : 0;
                 if (ov && more) bar_arrive(2, NTK);  // the list (and s_nc) may be overwritten
                 walk_emit<G, RC>(p, b, prev, P2w, clist, rowmask, (ov ? stage_ov : stage_bp) + warp * 32,
@@ -624,7 +648,6 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             }
             if (tid == PROD) s_nc = 0;  // every thread has read it (barrier 2)
         }
-        const FTile f = tile_of<TH0>(p, frame0, ntiles, g0 + k);
         const int ry0 = f.ty0 - HP - KR, rx0 = f.tx0 - G::L;
         const int py0 = f.ty0 - HP, px0 = f.tx0 - HX;
         float2* P2 = (float2*)(smem + (G::WS ? (k & 1) * G::SZ_P2 : 0));
@@ -632,13 +655,16 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             const int stid = tid - NWT;
             // ---- 0. the raw tile ----
             if (use_tma) {
-                bool done = false;
-                for (int it = 0; it < p.tma_spin && !done && !*(volatile int*)&s_fail; ++it)
-                    done = mbar_try_wait(&bar, k & 1);
-                if (!done && !*(volatile int*)&s_fail) {
-                    atomicOr(b.err, ERR_DEVICE_TIMEOUT);
-                    s_fail = 1;
+                // one thread waits for the copy, the stencil warps meet it
+                if (tid == PROD) {
+                    bool done = false;
+                    for (int it = 0; it < p.tma_spin && !done && !s_fail; ++it) done = mbar_try_wait(&bar, k & 1);
+                    if (!done && !s_fail) {
+                        atomicOr(b.err, ERR_DEVICE_TIMEOUT);
+                        s_fail = 1;
+                    }
                 }
+                bar_sync(4, NS);
             } else {
                 const unsigned short* fr = (const unsigned short*)b.frames + (size_t)f.t * H * W;
                 for (int i = stid; i < G::RH * G::US; i += NS) {
@@ -698,7 +724,8 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             //          preprocess_cols.wgsl:36-43), edge tiles only.  Boxcar column c is
             //          centred on frame column rx0 + KR + c and raw row r is frame row
             //          ry0 + r.  (h) the in-frame columns within KR of the left or right
-            //          edge are summed over reflected raw columns; (v) then each raw row
+            //          edge add their window's taps outside the frame, reflected into
+            //          it, to the row pass's zero-padded sums; (v) then each raw row
             //          within KR outside the top or bottom edge takes the boxcar row of
             //          its reflected row, so that the column pass's running sums give the
             //          reflect-padded vertical sums.  All sums are integers below 2^24,
@@ -706,7 +733,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             {
                 float* Bf = (float*)Bp;
                 const int cl0 = max(0, rx0 + KR), cl1 = min(KR, rx0 + KR + G::PWC);
-                const int cr0 = max(W - KR, rx0 + KR), cr1 = min(W, rx0 + KR + G::PWC);
+                const int cr0 = max(max(W - KR, cl1), rx0 + KR), cr1 = min(W, rx0 + KR + G::PWC);
                 const int nl = max(0, cl1 - cl0), nh = nl + max(0, cr1 - cr0);
                 const int rt0 = max(0, -KR - ry0), rt1 = max(rt0, min(G::RH, -ry0));
                 const int rb0 = max(0, H - ry0), rb1 = max(rb0, min(G::RH, H + KR - ry0));
@@ -716,11 +743,18 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
                     for (int i = stid; i < nh * G::RH; i += NS) {
                         const int j = i / G::RH, r = i - j * G::RH;
                         const int fc = j < nl ? cl0 + j : cr0 + (j - nl);
-                        float sum = 0.f;
+                        // the row pass summed the window over zeros outside the
+                        // frame; add the taps x < 0 and x >= W reflected to
+                        // frame columns -x - 1 and 2W - x - 1
+                        const unsigned short* Ur = U + r * G::US - rx0;  // frame column y at Ur[y]
+                        float corr = 0.f;
 #pragma unroll
-                        for (int t2 = 0; t2 < TAPS; ++t2)
-                            sum = sum + (float)U[r * G::US + clampi(reflect_once(fc - KR + t2, W) - rx0, 0, G::RW - 1)];
-                        Bf[(((r >> 1) * G::GPS + (fc - rx0 - KR)) << 1) + (r & 1)] = sum;
+                        for (int t = 0; t < KR; ++t) {
+                            if (t < KR - fc) corr = corr + (float)Ur[t];
+                            if (t < fc + KR - W + 1) corr = corr + (float)Ur[W - 1 - t];
+                        }
+                        float* d = Bf + ((((r >> 1) * G::GPS + (fc - rx0 - KR)) << 1) + (r & 1));
+                        *d = *d + corr;
                     }
                     if (nv > 0) bar_sync(5, NS);
                 }
@@ -741,7 +775,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         }
         // the raw tile is read: the next tile's copy lands during this one
         if (use_tma && tid == PROD && k + 1 < ntl && !s_fail) {
-            const FTile n = tile_of<TH0>(p, frame0, ntiles, g0 + k + 1);
+            const FTile n = next_tile<TH0>(p, f);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_expect_tx(&bar, (uint32_t)(G::RH * G::US * 2));
             if (!p.tma_withhold) tma_load_3d(U, &tmap, &bar, n.tx0 - G::L, n.ty0 - HP - KR, n.t);
@@ -893,6 +927,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
                 bal[m] = __ballot_sync(0xffffffffu, fl);
                 nc += __popc(bal[m]);
             }
+            const unsigned lt = (1u << lane) - 1u;
             int wbase = 0;
             if (lane == 0 && nc) wbase = atomicAdd(&s_nc, nc);
             wbase = __shfl_sync(0xffffffffu, wbase, 0);
@@ -905,6 +940,7 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
         }
         __syncthreads();
         prev = f;
+        f = next_tile<TH0>(p, f);
     }
     // a copy that ran out of the bounded wait gets a second one to land in
     // this CTA's shared memory before the CTA exits (no copy is issued after
