@@ -275,14 +275,14 @@ GT_API int gt_imsd(gt_ctx* ctx, const int64_t* ids, const int64_t* frames, const
  * Writes min(*nrows, out_rows) rows of the gt_batch_device columns to d_out
  * (device) and the row count to *nrows, on `stream` (a cudaStream_t, NULL =
  * default stream), returning after the work has finished: the call waits on
- * the stream and reads its row count back to the host, so it must not be
- * made while that stream is being captured into a CUDA graph.  Scratch
+ * the stream and reads its row count back to the host.  Scratch
  * lives in one 16 MiB __device__ array per GPU, held until the process
  * exits and shared by every call, which clears what must start at zero:
  * calls that overlap on one GPU (other streams, other host threads) race on
  * it and must be serialised by the caller.  The first call on a device looks
- * up that array's address (under a lock, so threads may call concurrently
- * for different GPUs).  Errors: gt_last_error(NULL) of the calling thread. */
+ * up that array's address and sets up the device (under a lock, so threads
+ * may call concurrently for different GPUs); make that first call before any
+ * stream capture.  Errors: gt_last_error(NULL) of the calling thread. */
 GT_API int gt_locate_frame_static(const void* d_frame, int dtype, int H, int W, const gt_params* params,
                                   float* d_out, int64_t out_rows, int64_t* nrows, void* stream);
 

@@ -9,8 +9,7 @@
 // needs lives in one file-scope __device__ array of kScratchBytes, which
 // each GPU that loads the library keeps until the process exits.  The call
 // waits for its own work on the caller's stream and reads its row count
-// back to the host, so it must not be made while that stream is being
-// captured into a CUDA graph.
+// back to the host.
 //
 // The kernels are the ones gt_batch_device launches for the same frame
 // (locate, fallback walk, ordering and separation filter, output rows);
