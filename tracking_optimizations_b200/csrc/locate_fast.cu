@@ -730,7 +730,8 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             //          its reflected row, so that the column pass's running sums give the
             //          reflect-padded vertical sums.  All sums are integers below 2^24,
             //          exact in any order. ----
-            {
+            // (only tiles whose raw rows or boxcar columns reach a frame edge)
+            if (rx0 < 0 || rx0 + KR + G::PWC > W - KR || ry0 < 0 || ry0 + G::RH > H) {
                 float* Bf = (float*)Bp;
                 const int cl0 = max(0, rx0 + KR), cl1 = min(KR, rx0 + KR + G::PWC);
                 const int cr0 = max(max(W - KR, cl1), rx0 + KR), cr1 = min(W, rx0 + KR + G::PWC);
@@ -918,11 +919,12 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             const bool col_in = f.tx0 + tc < W && !*(volatile int*)&s_fail;
             unsigned bal[FM];
             int nc = 0;
+            const int nin = col_in ? f.TH - tr0 : 0;  // rows m < nin are in the frame
 #pragma unroll
             for (int m = 0; m < FM; ++m) {
                 const int r = tr0 + m + HP;  // processed row of the centre
                 const float center = Pf[(((r >> 1) * G::P2S + tc + HX) << 1) + (r & 1)];
-                const bool in = col_in && tr0 + m < f.TH;
+                const bool in = m < nin;
                 const bool fl = in && cm[m] <= center && !(p.zero_skip && center == 0.f);
                 bal[m] = __ballot_sync(0xffffffffu, fl);
                 nc += __popc(bal[m]);
