@@ -920,12 +920,25 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             unsigned bal[FM];
             int nc = 0;
             const int nin = col_in ? f.TH - tr0 : 0;  // rows m < nin are in the frame
+            // the centres: processed rows tr0 + HP .. tr0 + HP + FM - 1, read
+            // as row pairs
+            constexpr int CPO = HP & 1, NCP = (CPO + FM + 1) / 2;
+            float cen[2 * NCP];
+            {
+                const int b0 = (tr0 + HP) >> 1;
+#pragma unroll
+                for (int k2 = 0; k2 < NCP; ++k2) {
+                    const float2 z = P2[(b0 + k2) * G::P2S + tc + HX];
+                    cen[2 * k2] = z.x;
+                    cen[2 * k2 + 1] = z.y;
+                }
+            }
+            // in-frame centres are >= 0: with zero_skip a centre must be > 0
+            const float zthr = p.zero_skip ? 0.f : -1.f;
 #pragma unroll
             for (int m = 0; m < FM; ++m) {
-                const int r = tr0 + m + HP;  // processed row of the centre
-                const float center = Pf[(((r >> 1) * G::P2S + tc + HX) << 1) + (r & 1)];
-                const bool in = m < nin;
-                const bool fl = in && cm[m] <= center && !(p.zero_skip && center == 0.f);
+                const float center = cen[CPO + m];
+                const bool fl = m < nin && cm[m] <= center && center > zthr;
                 bal[m] = __ballot_sync(0xffffffffu, fl);
                 nc += __popc(bal[m]);
             }
@@ -935,9 +948,11 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             wbase = __shfl_sync(0xffffffffu, wbase, 0);
 #pragma unroll
             for (int m = 0; m < FM; ++m) {
-                if ((bal[m] >> lane) & 1u)
-                    clist[wbase + __popc(bal[m] & lt)] = (unsigned short)((tr0 + m) * FT + tc);
-                wbase += __popc(bal[m]);
+                if (bal[m] != 0u) {  // warp-uniform: most rows list nothing
+                    if ((bal[m] >> lane) & 1u)
+                        clist[wbase + __popc(bal[m] & lt)] = (unsigned short)((tr0 + m) * FT + tc);
+                    wbase += __popc(bal[m]);
+                }
             }
         }
         __syncthreads();
