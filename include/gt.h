@@ -295,7 +295,7 @@ GT_API void gt_table_free(gt_table* table);
  *   "locate_tiles_per_cta"
  *                       output tiles located one after another by a CTA of
  *                       the specialised kernel, 1-64 (0 = the default: up to
- *                       8, as long as a launch keeps about four waves of CTAs)
+ *                       16, as long as a launch keeps about four waves of CTAs)
  *   "autotune"          0 = gt_batch_many_device keeps the configured tile rows
  *   "normalized_taps"   1 = Gaussian taps divided by their sum on the host and
  *                       no division in the passes (kernels.rs:86-97 gauss_1d,

@@ -1008,16 +1008,17 @@ bool fast_supported(int kr, int dd, int rc, int diameter) {
     return false;
 }
 
-// Tiles per CTA of a launch of `total` tiles: runs of up to 8 consecutive
-// tiles (a run overlaps each tile's walks with the next tile's row pass and
-// prefetches the next raw tile), as long as the launch keeps about four
-// waves of CTAs; p.tiles_per_cta > 0 sets it.
+// Tiles per CTA of a launch of `total` tiles: runs of up to 16 consecutive
+// tiles (within a run each tile's walks overlap the next tile's stencil
+// phases and the next raw tile is copied in behind the current one), as
+// long as the launch keeps about four waves of CTAs; p.tiles_per_cta > 0
+// sets it.
 int fast_tiles_per_cta(const LocParams& p, int total, int th) {
     if (p.tiles_per_cta > 0) return p.tiles_per_cta;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int slots = sms * (th == 32 ? 4 : 2);
-    return std::max(1, std::min(8, total / (4 * slots)));
+    return std::max(1, std::min(16, total / (4 * slots)));
 }
 
 // Launches the specialised kernel over frames [frame0, frame0 + grid.y),
