@@ -8,24 +8,28 @@
 // Specialised on (smoothing radius KR, dilation size DD, tile height TH0,
 // centroid radius RC with diameter 2*RC + 1), so the whole tile geometry is
 // known at compile time: every shared-memory offset is an immediate and
-// every loop has a constant trip count.  One CTA per (frame, TH0 x 64 output
-// tile), 256 or 512 threads:
+// every loop has a constant trip count.  A CTA (256 or 512 threads) takes a
+// run of consecutive TH0 x 64 output tiles; per tile:
 //   0. the uint16 tile plus halo is staged by one TMA load (zero fill
 //      outside the frame) into U[RH][US] (US >= RW: rows padded so that
-//      16-byte loads of consecutive row pairs spread over the banks);
+//      16-byte loads of consecutive row pairs spread over the banks); the
+//      next tile's load is issued once the row pass is done with U;
 //   1. (no separate conversion) the row pass reads row pairs of U with
 //      16-byte loads, turns each u16 into an exact float (2^23 + u, minus
 //      2^23) and filters 8 columns per thread (FFMA2 chains in tap order),
-//      Gaussian and boxcar -> Gp, Bp (row pairs);
+//      Gaussian and boxcar -> Gp, Bp (row pairs); tiles at a frame edge
+//      then repair the boxcar's reflect padding (the Gaussian pads with 0);
 //   2. column pass: a thread filters one column over 8 rows (4 row pairs),
 //      scales by the reciprocal of the Gaussian norm, subtracts the boxcar
-//      as fma(-box, 1/k^2, gauss) and clips at 0 -> P2 (row pairs);
+//      as fma(-box, 1/k^2, gauss) and clips at 0 -> P2 (row pairs); tiles at
+//      a frame edge then write -inf outside the frame;
 //   3. row max over the dilation window (register sliding max) -> RM2;
 //   4. column max of RM2 compared with the centre: the local maxima of a
 //      warp's rows are listed at once by per-row ballots into the CTA list;
-//   5. the list is walked one candidate per lane by as few warps as it
-//      needs; those warps compute the features and emit the records (ranks
-//      from per-row bit masks, one slot atomic per warp).
+//   5. the list is walked one candidate per lane by the walker warps, which
+//      compute the features and emit the records (ranks from per-row bit
+//      masks, one slot atomic per warp) while the other warps run the next
+//      tile's phases 0-3.
 // Row strides of the pair arrays are odd (in 8-byte units), so every
 // lane-per-row access is bank-conflict free.
 #include <cuda.h>
@@ -532,8 +536,9 @@ __device__ __forceinline__ void walk_emit(const LocParams& p, const MovieBufs& b
 }  // namespace
 
 // A CTA locates a run of consecutive tiles [g0, g0 + ntl) of the launch.
-// Warps 0 and 1 walk tile k - 1's candidates and emit its records (when it
-// has at most 64) while warps 2.. run tile k's row pass, and, with two
+// The walker warps [0, NWO) walk tile k - 1's candidates and emit its
+// records (when it has at most 32 NWO) while the stencil warps run tile k's
+// row pass, and, with two
 // processed planes (G::WS), its column pass and row max too: the warps meet
 // only for the column max and the list.  With one plane the walkers hold the
 // plane until the column pass.  A tile with more candidates is walked by as
@@ -541,8 +546,9 @@ __device__ __forceinline__ void walk_emit(const LocParams& p, const MovieBufs& b
 // copied in as soon as a row pass is done with the current one.  Named
 // barriers: 1 the walker warps, 2 "tile k - 1's list is read" (walkers
 // arrive, the stencil warps wait), 3 all warps before the column max (two
-// planes) or the column pass (one plane), 4 the stencil warps after a
-// staging without TMA, 5 the stencil warps between their phases.  A tile
+// planes) or the column pass (one plane), 4 the stencil warps once the raw
+// tile is in (one thread's wait for its copy, or their own staging without
+// TMA), 5 the stencil warps between their phases.  A tile
 // copy that does not land within the bounded wait sets ERR_DEVICE_TIMEOUT;
 // the CTA then issues no further copies, lists no candidates and finishes its
 // run (every barrier is still reached; the host discards the results).
