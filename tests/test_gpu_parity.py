@@ -271,3 +271,26 @@ def test_tables_alive_across_calls_keep_their_contents():
             del held[:2]  # released blocks go back to the pool and are reused
     for i, tab in held:
         np.testing.assert_array_equal(tab, want_a if i % 2 == 0 else want_b, err_msg=f"call {i}")
+
+
+def tiny_movie(H, W, seed):
+    """Three frames of H x W: read noise and a few bright Gaussian spots."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:H, 0:W]
+    mv = rng.normal(200.0, 8.0, (3, H, W))
+    for t in range(3):
+        for _ in range(max(2, H * W // 25)):
+            cy, cx = rng.uniform(0, H), rng.uniform(0, W)
+            mv[t] += 3000.0 * np.exp(-((yy - cy) ** 2 + (xx - cx) ** 2) / (2 * 1.2 ** 2))
+    return np.clip(mv, 0, 65535).astype(np.uint16)
+
+
+@pytest.mark.parametrize("diameter", [5, 7])
+@pytest.mark.parametrize("H,W", [(5, 40), (40, 5), (7, 7), (9, 13), (16, 8), (12, 30)])
+def test_tiny_frames(gpu, H, W, diameter):
+    """Frames narrower or shorter than a tile's halo: one tile covers the
+    frame, and a boxcar window can reach both frame edges (the specialised
+    kernel repairs the reflect padding of such tiles after its row pass)."""
+    mv = tiny_movie(H, W, H * 100 + W)
+    tab, _ = check(mv, diameter=diameter, minmass=50.0, search_range=3.0, cpu_processed=True)
+    assert _native.last_stats()["locate_kernel"] in (1, 2)
