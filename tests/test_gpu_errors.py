@@ -52,11 +52,16 @@ def test_subnet_budget_error_then_recovery(gpu):
     np.testing.assert_array_equal(gpu_tracking.link_rust(table, 5.0), want)
 
 
-def test_tile_copy_timeout_then_recovery(gpu):
+@pytest.mark.parametrize("per_cta", [0, 4])
+def test_tile_copy_timeout_then_recovery(gpu, per_cta):
+    """The withheld copy of a CTA's first tile runs out of its bounded wait;
+    with runs of 4 tiles per CTA the CTA then issues no further copies,
+    skips the later waits and still reaches every barrier."""
     movie = synth.make_movie(synth.scaled(synth.PLAIN_1000, frames=4, seed=9))
     params = dict(minmass=300.0, separation=8)
     want, _ = gpu_tracking.batch_rust(movie, 7, **params)
     assert _native.last_stats()["locate_kernel"] == 2  # the TMA-staged kernel ran
+    _native.set_option("locate_tiles_per_cta", per_cta)
     _native.set_option("test_withhold_tile_copy", 1)
     try:
         with pytest.raises(_native.GtError) as e:
@@ -64,5 +69,8 @@ def test_tile_copy_timeout_then_recovery(gpu):
         assert e.value.status == _native.GT_ERR_DEVICE_TIMEOUT
     finally:
         _native.set_option("test_withhold_tile_copy", 0)
-    got, _ = gpu_tracking.batch_rust(movie, 7, **params)
+    try:
+        got, _ = gpu_tracking.batch_rust(movie, 7, **params)
+    finally:
+        _native.set_option("locate_tiles_per_cta", 0)
     np.testing.assert_array_equal(got, want)
