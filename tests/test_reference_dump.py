@@ -5,8 +5,8 @@ tests/golden/make_reference_dump.py from gpu-tracking/masses.bin).
 The dump was made with Gaussian taps normalised on the host
 (kernels.rs:86-97); the oracle's ``normalized_taps`` form reproduces it bit
 for bit.  The live shaders normalise inside the passes instead
-(preprocess_rows.wgsl:52, preprocess_cols.wgsl:54); that form is held to the
-north-star mass tolerance (1e-4 relative) against the same dump.
+(preprocess_rows.wgsl:52, preprocess_cols.wgsl:54); that form is held to a
+mass tolerance of 1e-4 relative against the same dump.
 """
 import hashlib
 import os
