@@ -920,7 +920,6 @@ __global__ void __launch_bounds__(fast_threads(TH0), (TH0 == 32 ? 4 : 2))
             for (int i = 0; i < FM + DD - 1; ++i) v[i] = vv[i];
             float cm[FM];
             slide_max<DD, FM>(v, cm);
-            const float* Pf = (const float*)P2;
             // a tile whose copy ran out of its wait lists nothing
             const bool col_in = f.tx0 + tc < W && !*(volatile int*)&s_fail;
             unsigned bal[FM];
