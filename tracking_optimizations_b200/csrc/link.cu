@@ -148,6 +148,8 @@ __device__ bool solve_subnet(const LinkBufs& L, const int* dests, int nd, const 
 
 // One CTA per frame (grid-stride); frame t >= 1 links P(t-1) + M(t) to P(t).
 template <int NT>
+// only_dirty: 0 = every frame, else the dirty bit of the pass (frames whose
+// memory entries that pass changed).
 __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int tstride) {
     __shared__ int warp_tot[NT / 32];
     __shared__ int s_total;
@@ -161,7 +163,7 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
     const int pool = L.lsm_bytes / 4;
 
     for (int t = L.tb + t0; t < L.te; t += tstride) {
-        if (only_dirty && !__ldcg(L.dirty + t)) continue;
+        if (only_dirty && !(__ldcg(L.dirty + t) & only_dirty)) continue;
         const int nd = L.npart[t];
         int* pred = L.pred + L.off[t];
         if (t == 0) {
@@ -441,7 +443,7 @@ __device__ void link_frames_body(const LinkBufs& L, int only_dirty, int t0, int 
 // skipping trajectories present in frame t-1 and keeping the first entry of
 // each trajectory.  Marks frames whose M changed.
 template <int NT>
-__device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, int tstride) {
+__device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int wbit, int t0, int tstride) {
     __shared__ int warp_tot[NT / 32];
     __shared__ int s_total;
     __shared__ int s_diff;
@@ -577,11 +579,11 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
             }
             if (threadIdx.x == 0) {
                 L.mcount[t] = nk;
-                L.dirty[t] = 1;
+                atomicOr(L.dirty + t, wbit);
                 atomicAdd(ndirty, 1);
             }
         } else if (threadIdx.x == 0) {
-            L.dirty[t] = 0;
+            atomicAnd(L.dirty + t, ~wbit);
         }
         __syncthreads();
     }
@@ -606,8 +608,14 @@ __device__ void memory_body(const LinkBufs& L, int memory, int* ndirty, int t0, 
 // M(t) = the frame t-3 particles unused by t-2 and not the pred of a
 // frame t-1 particle, then the frame t-2 particles unused by t-1 (memory 1:
 // the latter only).  Marks frames whose M changed.
+// M(t) reads lnext of frames t-3 and t-2 and pred of frame t-1, which only
+// relinking frames t-2 and t-1 writes (lnext of a frame is written by the
+// link into the next frame), so from the second pass on (k > 1) a frame
+// whose frames t-1 and t-2 (memory 1: t-1) the previous pass did not relink
+// keeps its M.  Pass k marks with wbit = 1 << (k & 1) and reads the previous
+// pass's bit, so that concurrent marks never touch the bit being read.
 template <int NT>
-__device__ void memory_body_short(const LinkBufs& L, int memory, int* ndirty, int t0, int tstride) {
+__device__ void memory_body_short(const LinkBufs& L, int memory, int* ndirty, int k, int t0, int tstride) {
     __shared__ int warp_tot[NT / 32];
     __shared__ int s_total;
     __shared__ int s_diff;
@@ -615,9 +623,14 @@ __device__ void memory_body_short(const LinkBufs& L, int memory, int* ndirty, in
     const int slot = blockIdx.x;
     const int cap_p = L.cap_p;
     const int pool = L.lsm_bytes / 4;
+    const int wbit = 1 << (k & 1), pbit = 1 << ((k - 1) & 1);
     for (int t = L.tb + t0; t < L.te; t += tstride) {
         const int fbeg = max(0, t - 1 - memory), fend = t - 2;
         if (fend < fbeg) continue;
+        if (k > 1 && !(__ldcg(L.dirty + t - 1) & pbit) && !(memory == 2 && (__ldcg(L.dirty + t - 2) & pbit))) {
+            if (threadIdx.x == 0) atomicAnd(L.dirty + t, ~wbit);
+            continue;
+        }
         const int fo = (fend > fbeg) ? fbeg : -1;  // frame t-3 (memory 2)
         const int no = fo >= 0 ? L.npart[fo] : 0;
         const int nb = L.npart[fbeg], ne = L.npart[fend];
@@ -666,11 +679,11 @@ __device__ void memory_body_short(const LinkBufs& L, int memory, int* ndirty, in
             for (int j = threadIdx.x; j < nc; j += NT) ml[j] = ch[j];
             if (threadIdx.x == 0) {
                 L.mcount[t] = nc;
-                L.dirty[t] = 1;
+                atomicOr(L.dirty + t, wbit);
                 atomicAdd(ndirty, 1);
             }
         } else if (threadIdx.x == 0) {
-            L.dirty[t] = 0;
+            atomicAnd(L.dirty + t, ~wbit);
         }
         __syncthreads();
     }
@@ -778,12 +791,12 @@ __global__ void __launch_bounds__(NT, NT == NTL ? 4 : 1) link_fixpoint_kernel(Li
                 grid.sync();
             }
             if (stamp) { const unsigned long long t = gtimer(); acc[1] += t - t0; t0 = t; }
-            if (short_mem) memory_body_short<NT>(L, memory, ndirty + k, blockIdx.x, gridDim.x);
-            else memory_body<NT>(L, memory, ndirty + k, blockIdx.x, gridDim.x);
+            if (short_mem) memory_body_short<NT>(L, memory, ndirty + k, k, blockIdx.x, gridDim.x);
+            else memory_body<NT>(L, memory, ndirty + k, 1 << (k & 1), blockIdx.x, gridDim.x);
             grid.sync();
             if (stamp) { const unsigned long long t = gtimer(); acc[2] += t - t0; t0 = t; }
             if (*(volatile int*)(ndirty + k) == 0) break;
-            link_frames_body<NT>(L, 1, blockIdx.x, gridDim.x);
+            link_frames_body<NT>(L, 1 << (k & 1), blockIdx.x, gridDim.x);
         }
     }
     grid.sync();
@@ -853,15 +866,15 @@ __global__ void __launch_bounds__(NTL, 4) link_fixpoint_multi_kernel(const LinkB
             grid.sync();
             for (int m = 0; m < nm; ++m) {
                 if (!active(m, k)) continue;
-                if (memory[m] <= 2) memory_body_short<NTL>(Ls[m], memory[m], ndirty + k * nm + m, t0_of(m), G);
-                else memory_body<NTL>(Ls[m], memory[m], ndirty + k * nm + m, t0_of(m), G);
+                if (memory[m] <= 2) memory_body_short<NTL>(Ls[m], memory[m], ndirty + k * nm + m, k, t0_of(m), G);
+                else memory_body<NTL>(Ls[m], memory[m], ndirty + k * nm + m, 1 << (k & 1), t0_of(m), G);
             }
             grid.sync();
             int total = 0;
             for (int m = 0; m < nm; ++m) total += *(volatile int*)(ndirty + k * nm + m);
             if (total == 0) break;
             for (int m = 0; m < nm; ++m)
-                if (*(volatile int*)(ndirty + k * nm + m) > 0) link_frames_body<NTL>(Ls[m], 1, t0_of(m), G);
+                if (*(volatile int*)(ndirty + k * nm + m) > 0) link_frames_body<NTL>(Ls[m], 1 << (k & 1), t0_of(m), G);
         }
     }
     grid.sync();
